@@ -1,0 +1,131 @@
+// Host side of the B200 full-field solve: the reference cache held on the
+// device and run_full_field over it.
+//
+// Mirrors Semper::pipeline::ReferenceCache (include/semper/pipeline.hpp:35-64)
+// and run_full_field / run_full_field_impl (src/pipeline/full_field_solver.cpp:
+// 44-59, 141-586) with a raw 8-bit gray view in place of cv::Mat. Every
+// data-parallel stage runs as a kernel; the orchestration between them (the
+// lattice median test, routing, Delaunay mesh, Path B's deterministic rounds,
+// metrics) runs here, on exactly the reference's rules.
+#pragma once
+#include <atomic>
+#include <cstdint>
+#include <functional>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../kernels/dic_types.h"
+
+namespace semper_b200 {
+
+struct CudaError : std::runtime_error {
+    explicit CudaError(const std::string& s) : std::runtime_error(s) {}
+};
+
+void check(cudaError_t e, const char* what);
+
+// A growable device allocation.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void ensure(size_t count) {
+        if (count <= n && p) return;
+        release();
+        if (count == 0) count = 1;
+        check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct Params {
+    int rect_x = 0, rect_y = 0, rect_w = 0, rect_h = 0, step = 0, subset_size = 0, strain_window = 0;
+    bool six = false;
+};
+
+using Progress = std::function<void(int)>;
+
+// The per-node state a caller can take after the solve (FieldCapture,
+// src/pipeline/full_field_internal.hpp:247-261).
+struct Capture {
+    int gridW = 0, gridH = 0, rect_x = 0, rect_y = 0, step = 0, attempted = 0;
+    std::vector<float> u, v, ux, uy, vx, vy, corr;
+    std::vector<uint8_t> solved;
+};
+
+// Timings of one solve's device phases, measured with CUDA events on the
+// engine's stream (ms).
+struct PhaseTimes {
+    float prep = 0, pool = 0, seed = 0, mesh = 0, path_a = 0, path_b = 0, strain = 0, total = 0;
+    long long icgn_iters = 0;   // IC-GN iterations of every subset solve
+    long long pixel_iters = 0;  // subset pixels x iterations (the IC-GN work)
+    int path_a_tasks = 0;
+};
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+    Engine(const Engine&) = delete;
+    Engine& operator=(const Engine&) = delete;
+
+    // ReferenceCache::set_from_gray: w x h gray bytes (host), optional mask of
+    // the same size (host). The previous reference is dropped first.
+    int set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask);
+    // The deformed frame of the last solve becomes the reference
+    // (ReferenceCache::adopt, src/pipeline/reference_cache.cpp:82-108): its
+    // prepared planes are taken over on the device.
+    int adopt_last_deformed(const uint8_t* mask);
+    void reset();
+    bool has_reference() const { return has_ref_; }
+    int width() const { return W_; }
+    int height() const { return H_; }
+
+    // run_full_field over a host deformed image (w x h bytes): host in, host out.
+    int run(const uint8_t* def_gray, const uint8_t* mask, Params p, float* out, int capacity, float* metrics,
+            int metrics_len, const double* model_H = nullptr, Progress progress = nullptr,
+            Capture* capture = nullptr);
+
+    // The same with the deformed image already on the device and the packed
+    // output left on the device (d_out, capacity floats).
+    int run_device(const uint8_t* d_def, const uint8_t* mask, Params p, float* d_out, int capacity,
+                   float* metrics, int metrics_len, const double* model_H = nullptr, Progress progress = nullptr,
+                   Capture* capture = nullptr);
+
+    void request_cancel() { h_cancel_[0] = 1; }
+    void clear_cancel() { h_cancel_[0] = 0; }
+    bool cancel_requested() const { return h_cancel_[0] != 0; }
+
+    cudaStream_t stream() const { return stream_; }
+    const PhaseTimes& last_times() const { return times_; }
+    // Grid blocks of the persistent solve kernel (0: automatic).
+    void set_solve_blocks(int b) { solve_blocks_ = b; }
+
+    struct Impl;
+
+private:
+    std::unique_ptr<Impl> impl_;
+    cudaStream_t stream_ = nullptr;
+    volatile int* h_cancel_ = nullptr;  // host-mapped pinned flag
+    int* d_cancel_ = nullptr;
+    bool has_ref_ = false;
+    int W_ = 0, H_ = 0;
+    int solve_blocks_ = 0;
+    PhaseTimes times_;
+    friend struct Impl;
+};
+
+}  // namespace semper_b200

@@ -1,0 +1,257 @@
+// The C ABI (include/semper_c.h) over the device engine: a thin translation,
+// no algorithm. Restates adapters/c/semper_c.cpp:25-238 on this library's
+// engine — per-handle busy guard, per-handle cancel token with the reference's
+// cancel window (include/semper/cancel.hpp:53-110), and an exception barrier
+// at every entry (include/semper/guarded_call.hpp:22-44).
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <vector>
+
+#include "../../../include/semper_c.h"
+#include "engine.hpp"
+#include "incremental.hpp"
+
+using semper_b200::Engine;
+using semper_b200::IncrementalSession;
+using semper_b200::Params;
+
+namespace {
+
+template <class R, class F>
+R guarded(R on_error, F&& body) noexcept {
+    try {
+        return body();
+    } catch (...) {
+        return on_error;
+    }
+}
+
+// CancelToken + CancelScope on the engine's mapped flag.
+struct CancelWindow {
+    std::atomic<bool> open{false};
+};
+
+class HandleCall {
+public:
+    explicit HandleCall(std::atomic<bool>& b) noexcept : busy_(b), owned_(!b.exchange(true, std::memory_order_acquire)) {}
+    ~HandleCall() {
+        if (owned_) busy_.store(false, std::memory_order_release);
+    }
+    bool owned() const { return owned_; }
+
+private:
+    std::atomic<bool>& busy_;
+    bool owned_;
+};
+
+Params to_params(const semper_params* p) {
+    Params q;
+    q.rect_x = p->rect_x;
+    q.rect_y = p->rect_y;
+    q.rect_w = p->rect_w;
+    q.rect_h = p->rect_h;
+    q.step = p->step;
+    q.subset_size = p->subset_size;
+    q.strain_window = p->strain_window;
+    q.six = p->use_6x6_interpolator != 0;
+    return q;
+}
+
+// io::decode_gray for raw buffers (src/io/image_codec.cpp:126-160): ALPHA_8
+// when len == w*h, RGBA when len == 4*w*h (BT.601 luma, rounded). Encoded
+// images are not decoded by this build: empty result.
+bool decode_raw(const uint8_t* data, size_t len, int w, int h, std::vector<uint8_t>& out) {
+    if (!data || len == 0 || w <= 0 || h <= 0) return false;
+    const uint64_t px = (uint64_t)w * (uint64_t)h;
+    if (px > (uint64_t)INT32_MAX) return false;
+    if ((uint64_t)len == px) {
+        out.assign(data, data + px);
+        return true;
+    }
+    if ((uint64_t)len == 4 * px) {
+        out.resize(px);
+        for (uint64_t i = 0; i < px; ++i) {
+            const double y = 0.299 * data[4 * i] + 0.587 * data[4 * i + 1] + 0.114 * data[4 * i + 2];
+            const long r = std::lround(y);
+            out[i] = (uint8_t)(r < 0 ? 0 : (r > 255 ? 255 : r));
+        }
+        return true;
+    }
+    return false;
+}
+
+// decode_mask: no bytes is no mask; bytes that do not decode are an error.
+bool decode_mask(const uint8_t* m, size_t len, int w, int h, std::vector<uint8_t>& out, bool& has) {
+    has = false;
+    if (m == nullptr || len == 0) return true;
+    if (!decode_raw(m, len, w, h, out)) return false;
+    has = true;
+    return true;
+}
+
+}  // namespace
+
+struct semper_engine {
+    Engine engine;
+    CancelWindow window;
+    std::atomic<bool> busy{false};
+};
+
+struct semper_incremental {
+    std::unique_ptr<IncrementalSession> session;
+    CancelWindow window;
+    int width = 0, height = 0;
+    std::atomic<bool> busy{false};
+};
+
+namespace {
+
+// CancelToken::begin / enter / end on an engine's flag.
+void window_begin(Engine& e, CancelWindow& w) {
+    e.clear_cancel();
+    w.open.store(true, std::memory_order_release);
+}
+void window_enter(Engine& e, CancelWindow& w) {
+    if (!w.open.exchange(false, std::memory_order_acq_rel)) e.clear_cancel();
+}
+struct WindowScope {
+    Engine& e;
+    CancelWindow& w;
+    WindowScope(Engine& e_, CancelWindow& w_) : e(e_), w(w_) { window_begin(e, w); }
+    ~WindowScope() { w.open.store(false, std::memory_order_release); }
+};
+
+}  // namespace
+
+extern "C" {
+
+SEMPER_C_API semper_engine* semper_create(void) {
+    return guarded<semper_engine*>(nullptr, [] { return new semper_engine(); });
+}
+
+SEMPER_C_API void semper_destroy(semper_engine* eng) { delete eng; }
+
+SEMPER_C_API int semper_set_reference(semper_engine* eng, const uint8_t* img, size_t img_len, const uint8_t* mask,
+                                      size_t mask_len, int expected_w, int expected_h) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    guarded(0, [&] {
+        eng->engine.reset();
+        return 0;
+    });
+    if (img == nullptr || img_len == 0) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        std::vector<uint8_t> ref, m;
+        if (!decode_raw(img, img_len, expected_w, expected_h, ref)) return SEMPER_ERR_INIT;
+        bool has_mask = false;
+        if (!decode_mask(mask, mask_len, expected_w, expected_h, m, has_mask)) return SEMPER_ERR_INIT;
+        return eng->engine.set_reference(ref.data(), expected_w, expected_h, has_mask ? m.data() : nullptr) == 0
+                   ? 0
+                   : SEMPER_ERR_INIT;
+    });
+}
+
+SEMPER_C_API int semper_run(semper_engine* eng, const uint8_t* def, size_t def_len, const uint8_t* mask,
+                            size_t mask_len, const semper_params* params, float* out, int out_capacity,
+                            float* metrics, int metrics_len, semper_progress_cb cb, void* user) {
+    if (eng == nullptr || def == nullptr || def_len == 0 || params == nullptr || out == nullptr || out_capacity < 0)
+        return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        WindowScope scope(eng->engine, eng->window);
+        if (!eng->engine.has_reference()) return SEMPER_ERR_INIT;
+        const int w = eng->engine.width(), h = eng->engine.height();
+        std::vector<uint8_t> d, m;
+        if (!decode_raw(def, def_len, w, h, d)) return SEMPER_ERR_INIT;
+        bool has_mask = false;
+        if (!decode_mask(mask, mask_len, w, h, m, has_mask)) return SEMPER_ERR_INIT;
+        semper_b200::Progress progress;
+        if (cb) progress = [cb, user](int pct) { cb(pct, user); };
+        window_enter(eng->engine, eng->window);
+        return eng->engine.run(d.data(), has_mask ? m.data() : nullptr, to_params(params), out, out_capacity,
+                               metrics, metrics_len, nullptr, progress);
+    });
+}
+
+SEMPER_C_API void semper_cancel(semper_engine* eng) {
+    if (eng != nullptr) eng->engine.request_cancel();
+}
+
+SEMPER_C_API const char* semper_version(void) { return "0.6.1"; }
+
+SEMPER_C_API semper_incremental* semper_incremental_create(void) {
+    return guarded<semper_incremental*>(nullptr, [] {
+        auto* inc = new semper_incremental();
+        inc->session.reset(new IncrementalSession());
+        return inc;
+    });
+}
+
+SEMPER_C_API void semper_incremental_destroy(semper_incremental* inc) { delete inc; }
+
+SEMPER_C_API int semper_incremental_init(semper_incremental* inc, const uint8_t* ref, size_t ref_len,
+                                         const uint8_t* mask, size_t mask_len, int expected_w, int expected_h,
+                                         const semper_params* params, int32_t update_interval) {
+    if (inc == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(inc->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    guarded(0, [&] {
+        inc->session->reset();
+        return 0;
+    });
+    inc->width = inc->height = 0;
+    if (ref == nullptr || ref_len == 0 || params == nullptr) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        std::vector<uint8_t> r, m;
+        if (!decode_raw(ref, ref_len, expected_w, expected_h, r)) return SEMPER_ERR_INIT;
+        bool has_mask = false;
+        if (!decode_mask(mask, mask_len, expected_w, expected_h, m, has_mask)) return SEMPER_ERR_INIT;
+        const int rc = inc->session->init(r.data(), expected_w, expected_h, has_mask ? m.data() : nullptr,
+                                          to_params(params), update_interval);
+        inc->width = rc == 0 ? expected_w : 0;
+        inc->height = rc == 0 ? expected_h : 0;
+        return rc;
+    });
+}
+
+SEMPER_C_API int semper_incremental_process(semper_incremental* inc, const uint8_t* def, size_t def_len, float* out,
+                                            int out_capacity, float* metrics, int metrics_len,
+                                            semper_incremental_info* info, semper_progress_cb cb, void* user) {
+    if (inc == nullptr || def == nullptr || def_len == 0 || out == nullptr || out_capacity < 0)
+        return SEMPER_ERR_INIT;
+    HandleCall call(inc->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    if (!inc->session->initialized()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        Engine& e = inc->session->engine();
+        WindowScope scope(e, inc->window);
+        std::vector<uint8_t> d;
+        if (!decode_raw(def, def_len, inc->width, inc->height, d)) return SEMPER_ERR_INIT;
+        semper_b200::Progress progress;
+        if (cb) progress = [cb, user](int pct) { cb(pct, user); };
+        window_enter(e, inc->window);
+        semper_b200::FrameInfo fi;
+        const int rc = inc->session->process(d.data(), out, out_capacity, metrics, metrics_len, progress, &fi);
+        if (info != nullptr && rc >= 0) {
+            info->reference_frame = fi.reference_frame;
+            info->reference_updated = fi.reference_updated ? 1 : 0;
+            info->tracked_points = fi.tracked_points;
+            info->frame0_points = fi.frame0_points;
+            info->taylor_fallbacks = fi.taylor_fallbacks;
+            info->lost_this_frame = fi.lost_this_frame;
+        }
+        return rc;
+    });
+}
+
+SEMPER_C_API void semper_incremental_cancel(semper_incremental* inc) {
+    if (inc != nullptr && inc->session) inc->session->engine().request_cancel();
+}
+
+}  // extern "C"

@@ -1,0 +1,190 @@
+// Device building blocks shared by the DIC kernels (sm_100a).
+//
+// Arithmetic contract. Every kernel file is compiled with -fmad=false, so no
+// multiply-add is fused unless written as __fmaf_rn / __fma_rn here. Subset
+// reductions put pixel i (row-major in the subset) in lane i % 32, accumulate
+// in increasing i, and finish with an xor butterfly; IEEE addition being
+// commutative, every lane ends with the same bits. The CPU restatement used by
+// the tests follows the same contract, so results agree bit for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace dic {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ float wsum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = __fadd_rn(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = __dadd_rn(v, __shfl_xor_sync(kFull, v, o));
+    return v;
+}
+__device__ __forceinline__ int wsum(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+__device__ __forceinline__ bool finite_f(float f) {
+    return (__float_as_uint(f) & 0x7f800000u) != 0x7f800000u;
+}
+__device__ __forceinline__ bool finite_d(double d) {
+    return ((unsigned long long)__double_as_longlong(d) & 0x7ff0000000000000ull) != 0x7ff0000000000000ull;
+}
+
+// Catmull-Rom weights (src/math/image_processor.cpp:188-195) with the fused
+// products of the contract.
+__device__ __forceinline__ void cubic_weights(float s, float w[4]) {
+    const float s2 = s * s, s3 = s2 * s;
+    w[0] = __fmaf_rn(-0.5f, s, __fmaf_rn(-0.5f, s3, s2));
+    w[1] = __fmaf_rn(-2.5f, s2, __fmaf_rn(1.5f, s3, 1.0f));
+    w[2] = __fmaf_rn(0.5f, s, __fmaf_rn(-1.5f, s3, 2.0f * s2));
+    w[3] = __fmaf_rn(0.5f, s3, -0.5f * s2);
+}
+
+// Keys 4th-order zones (image_processor.cpp:70-82).
+__device__ __forceinline__ float keys_f0(float s) {
+    const float s2 = s * s, s3 = s2 * s;
+    return __fmaf_rn(4.0f / 3.0f, s3, __fmaf_rn(-7.0f / 3.0f, s2, 1.0f));
+}
+__device__ __forceinline__ float keys_f1(float s) {
+    const float s2 = s * s, s3 = s2 * s;
+    return __fmaf_rn(-7.0f / 12.0f, s3, __fmaf_rn(3.0f, s2, __fmaf_rn(-59.0f / 12.0f, s, 2.5f)));
+}
+__device__ __forceinline__ float keys_f2(float s) {
+    const float s2 = s * s, s3 = s2 * s;
+    return __fmaf_rn(1.0f / 12.0f, s3, __fmaf_rn(-2.0f / 3.0f, s2, __fmaf_rn(7.0f / 4.0f, s, -1.5f)));
+}
+__device__ __forceinline__ void keys6_weights(float d, float w[6]) {
+    w[0] = keys_f2(d + 2.0f);
+    w[1] = keys_f1(d + 1.0f);
+    w[2] = keys_f0(d);
+    w[3] = keys_f0(1.0f - d);
+    w[4] = keys_f1(2.0f - d);
+    w[5] = keys_f2(3.0f - d);
+}
+
+// Interpolated value at (xi + dx, yi + dy) from a row-major float plane with
+// row pitch `pitch` (elements); base points at element (0, 0) of the plane.
+__device__ __forceinline__ float interp4(const float* __restrict__ base, int pitch, int xi, int yi,
+                                         float dx, float dy) {
+    float wx[4], wy[4];
+    cubic_weights(dx, wx);
+    cubic_weights(dy, wy);
+    const float* r = base + (size_t)(yi - 1) * pitch + (xi - 1);
+    float val = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float* q = r + (size_t)j * pitch;
+        float rv = __ldg(q) * wx[0];
+        rv = __fmaf_rn(__ldg(q + 1), wx[1], rv);
+        rv = __fmaf_rn(__ldg(q + 2), wx[2], rv);
+        rv = __fmaf_rn(__ldg(q + 3), wx[3], rv);
+        val = (j == 0) ? rv * wy[0] : __fmaf_rn(rv, wy[j], val);
+    }
+    return val;
+}
+
+__device__ __forceinline__ float interp6(const float* __restrict__ base, int pitch, int xi, int yi,
+                                         float dx, float dy) {
+    float wx[6], wy[6];
+    keys6_weights(dx, wx);
+    keys6_weights(dy, wy);
+    const float* r = base + (size_t)(yi - 2) * pitch + (xi - 2);
+    float val = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const float* q = r + (size_t)j * pitch;
+        float rv = __ldg(q) * wx[0];
+#pragma unroll
+        for (int i = 1; i < 6; ++i) rv = __fmaf_rn(__ldg(q + i), wx[i], rv);
+        val = (j == 0) ? rv * wy[0] : __fmaf_rn(rv, wy[j], val);
+    }
+    return val;
+}
+
+// The 6x6 FP64 helpers of the Hessian: Cholesky, explicit inverse, and the
+// scaled 1-norm reciprocal condition (src/math/hessian.hpp:40-52).
+static __device__ __noinline__ bool cholesky6(const double A[6][6], double L[6][6]) {
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) L[i][j] = 0.0;
+    for (int j = 0; j < 6; ++j) {
+        double s = A[j][j];
+        for (int k = 0; k < j; ++k) s = s - L[j][k] * L[j][k];
+        if (!(s > 0.0) || !finite_d(s)) return false;
+        const double d = sqrt(s);
+        L[j][j] = d;
+        for (int i = j + 1; i < 6; ++i) {
+            double t = A[i][j];
+            for (int k = 0; k < j; ++k) t = t - L[i][k] * L[j][k];
+            L[i][j] = t / d;
+        }
+    }
+    return true;
+}
+
+static __device__ __noinline__ bool inverse6(const double A[6][6], double Ai[6][6]) {
+    double L[6][6];
+    if (!cholesky6(A, L)) return false;
+    double Li[6][6];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) Li[i][j] = 0.0;
+    for (int c = 0; c < 6; ++c) {
+        Li[c][c] = 1.0 / L[c][c];
+        for (int i = c + 1; i < 6; ++i) {
+            double t = 0.0;
+            for (int k = c; k < i; ++k) t = t + L[i][k] * Li[k][c];
+            Li[i][c] = -t / L[i][i];
+        }
+    }
+    bool ok = true;
+    for (int r = 0; r < 6; ++r)
+        for (int c = r; c < 6; ++c) {
+            double t = 0.0;
+            for (int k = c; k < 6; ++k) t = t + Li[k][r] * Li[k][c];
+            Ai[r][c] = t;
+            Ai[c][r] = t;
+            ok = ok && finite_d(t);
+        }
+    return ok;
+}
+
+static __device__ __noinline__ bool well_conditioned(const double H[6][6], int half) {
+    const double s = half > 1 ? 1.0 / (double)half : 1.0;
+    const double d[6] = {1.0, 1.0, s, s, s, s};
+    double Hn[6][6], Hi[6][6];
+    for (int r = 0; r < 6; ++r)
+        for (int c = 0; c < 6; ++c) {
+            Hn[r][c] = (d[r] * H[r][c]) * d[c];
+            if (!finite_d(Hn[r][c])) return false;
+        }
+    if (!inverse6(Hn, Hi)) return false;
+    double na = 0.0, ni = 0.0;
+    for (int c = 0; c < 6; ++c) {
+        double a = 0.0, b = 0.0;
+        for (int r = 0; r < 6; ++r) {
+            a = a + fabs(Hn[r][c]);
+            b = b + fabs(Hi[r][c]);
+        }
+        na = fmax(na, a);
+        ni = fmax(ni, b);
+    }
+    return 1.0 / (na * ni) > (double)1e-6f;
+}
+
+static __device__ __noinline__ bool cond2x2_ok(const double H[6][6]) {
+    const double det = H[0][0] * H[1][1] - H[1][0] * H[0][1];
+    const double nrm = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[1][0] * H[1][0] + H[1][1] * H[1][1];
+    const double cond = fabs(det) > 1e-12 ? nrm / fabs(det) : 1.0e13;
+    return !(cond > 1.0e12);
+}
+
+// Index of (r, c), r <= c, in the 21-entry upper triangle (row-major).
+__host__ __device__ constexpr int tri21(int r, int c) { return r * 6 - (r * (r - 1)) / 2 + (c - r); }
+
+}  // namespace dic

@@ -1,0 +1,251 @@
+// Reference/deformed image preparation, the grid validity scan, and the
+// per-node Hessian pool.
+//
+//   image pass      Image::Image + prepare_data(false) (src/math/image_processor.cpp:9-24,54-63)
+//                   + stamp_ghost_wall (src/pipeline/reference_cache.cpp:18-35)
+//   grid scan       src/pipeline/full_field_solver.cpp:266-318
+//   Hessian pool    SubsetPrecomputer::compute_hessian_only (src/math/subset_precomputer.cpp:42-149)
+//                   + hessian::well_conditioned (src/math/hessian.hpp:40-52), FP64
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "prep.cuh"
+
+namespace dic {
+
+namespace {
+
+// One thread per 4 horizontally adjacent pixels: u8 -> f32 intensity and the
+// 4th-order central-difference gradients (zero within 2 px of the border),
+// then the Ghost Wall where the mask is below 128. Integer numerators make
+// the gradient the correctly rounded quotient in any order. Stores are float4
+// when the row pitch allows it (W % 4 == 0), scalar otherwise.
+__global__ void image_kernel(const uint8_t* __restrict__ px, const uint8_t* __restrict__ mask, int W,
+                             int H, float* __restrict__ I, float* __restrict__ gx, float* __restrict__ gy) {
+    const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    const int y = blockIdx.y;
+    if (x0 >= W || y >= H) return;
+    const size_t row = (size_t)y * W;
+    float vi[4], vx[4], vy[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int x = x0 + k;
+        vi[k] = vx[k] = vy[k] = 0.0f;
+        if (x >= W) continue;
+        const size_t p = row + x;
+        vi[k] = (float)__ldg(px + p);
+        if (x >= 2 && x < W - 2 && y >= 2 && y < H - 2) {
+            const int nx = -(int)__ldg(px + p + 2) + 8 * (int)__ldg(px + p + 1) - 8 * (int)__ldg(px + p - 1) +
+                           (int)__ldg(px + p - 2);
+            const int ny = -(int)__ldg(px + p + 2 * (size_t)W) + 8 * (int)__ldg(px + p + W) -
+                           8 * (int)__ldg(px + p - W) + (int)__ldg(px + p - 2 * (size_t)W);
+            vx[k] = __fdiv_rn((float)nx, 12.0f);
+            vy[k] = __fdiv_rn((float)ny, 12.0f);
+        }
+        if (mask && __ldg(mask + p) < 128) vi[k] = -10.0f;
+    }
+    if ((W & 3) == 0) {
+        reinterpret_cast<float4*>(I + row)[x0 >> 2] = make_float4(vi[0], vi[1], vi[2], vi[3]);
+        reinterpret_cast<float4*>(gx + row)[x0 >> 2] = make_float4(vx[0], vx[1], vx[2], vx[3]);
+        reinterpret_cast<float4*>(gy + row)[x0 >> 2] = make_float4(vy[0], vy[1], vy[2], vy[3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (x0 + k >= W) break;
+            I[row + x0 + k] = vi[k];
+            gx[row + x0 + k] = vx[k];
+            gy[row + x0 + k] = vy[k];
+        }
+    }
+}
+
+// One warp per grid node: skip within half + 19 px of the border, or when any
+// subset pixel is masked (< 128).
+__global__ void scan_kernel(const uint8_t* __restrict__ mask, int W, int H, int gridW, int gridH, int rect_x,
+                            int rect_y, int step, int dim, uint8_t* __restrict__ skip, int* __restrict__ n_valid) {
+    const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (node >= gridW * gridH) return;
+    const int gx = node % gridW, gy = node / gridW;
+    const int rx = rect_x + gx * step, ry = rect_y + gy * step;
+    const int hs = dim / 2, buf = hs + 4 + 15;
+    bool s = rx - buf < 0 || rx + buf >= W || ry - buf < 0 || ry + buf >= H;
+    if (!s && mask) {
+        int bad = 0;
+        for (int i = lane; i < dim * dim; i += 32) {
+            const int dy = i / dim - hs, dx = i % dim - hs;
+            if (__ldg(mask + (size_t)(ry + dy) * W + rx + dx) < 128) bad = 1;
+        }
+        s = __any_sync(kFull, bad) != 0;
+    }
+    if (lane == 0) {
+        skip[node] = s ? 1 : 0;
+        if (!s) atomicAdd(n_valid, 1);
+    }
+}
+
+// One warp per node of the pool: mean and std over non-Ghost pixels (FP32,
+// lane partial sums + butterfly), the 21-entry Gauss-Newton Hessian (FP64),
+// then the 2x2 and scaled-rcond checks on lane 0.
+__global__ void pool_kernel(const float* __restrict__ I, const float* __restrict__ Gx,
+                            const float* __restrict__ Gy, int W, int H, const uint8_t* __restrict__ skip,
+                            int gridW, int gridH, int rect_x, int rect_y, int step, int dim, int lm,
+                            uint8_t* __restrict__ valid, float2* __restrict__ ms, double* __restrict__ H21,
+                            double* __restrict__ Hs21) {
+    const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (node >= gridW * gridH) return;
+    const int half = dim / 2, n = dim * dim;
+    const int cx = rect_x + (node % gridW) * step, cy = rect_y + (node / gridW) * step;
+    const bool ok_dim = dim >= 3 && (dim & 1);
+    const bool on = cx - half >= 0 && cx + half < W && cy - half >= 0 && cy + half < H;
+    if ((skip && skip[node]) || !ok_dim || !on) {
+        if (lane == 0) {
+            valid[node] = 0;
+            ms[node] = make_float2(0.0f, 1.0f);
+        }
+        if (lane < 21) {
+            if (H21) H21[(size_t)node * 21 + lane] = 0.0;
+            Hs21[(size_t)node * 21 + lane] = 0.0;
+        }
+        return;
+    }
+    const size_t base = (size_t)(cy - half) * W + (cx - half);
+    const int q = 32 / dim, r = 32 - q * dim;
+
+    float part = 0.0f;
+    int cnt = 0;
+    {
+        int row = lane / dim, col = lane - row * dim;
+        for (int i = lane; i < n; i += 32) {
+            const float v = __ldg(I + base + (size_t)row * W + col);
+            if (!(v < -5.0f)) {
+                part = part + v;
+                ++cnt;
+            }
+            col += r; row += q;
+            if (col >= dim) { col -= dim; ++row; }
+        }
+    }
+    cnt = wsum(cnt);
+    const float sum = wsum(part);
+    if ((float)cnt < (float)n * 0.5f) {
+        if (lane == 0) {
+            valid[node] = 0;
+            ms[node] = make_float2(0.0f, 1.0f);
+        }
+        if (lane < 21) {
+            if (H21) H21[(size_t)node * 21 + lane] = 0.0;
+            Hs21[(size_t)node * 21 + lane] = 0.0;
+        }
+        return;
+    }
+    const float mean = sum / (float)cnt;
+    part = 0.0f;
+    {
+        int row = lane / dim, col = lane - row * dim;
+        for (int i = lane; i < n; i += 32) {
+            const float v = __ldg(I + base + (size_t)row * W + col);
+            if (!(v < -5.0f)) {
+                const float d = v - mean;
+                part = __fmaf_rn(d, d, part);
+            }
+            col += r; row += q;
+            if (col >= dim) { col -= dim; ++row; }
+        }
+    }
+    float sd = sqrtf(wsum(part) / (float)cnt);
+    if (sd < 1e-5f) sd = 1.0f;
+    const float inv = 1.0f / sd;
+
+    double hp[21];
+#pragma unroll
+    for (int k = 0; k < 21; ++k) hp[k] = 0.0;
+    {
+        int row = lane / dim, col = lane - row * dim;
+        for (int i = lane; i < n; i += 32) {
+            const size_t p = base + (size_t)row * W + col;
+            if (!(__ldg(I + p) < -5.0f)) {
+                const float g0 = __ldg(Gx + p) * inv, g1 = __ldg(Gy + p) * inv;
+                const float fx = (float)(col - half), fy = (float)(row - half);
+                const double s[6] = {(double)g0, (double)g1, (double)(g0 * fx), (double)(g0 * fy),
+                                     (double)(g1 * fx), (double)(g1 * fy)};
+                int k = 0;
+#pragma unroll
+                for (int a = 0; a < 6; ++a)
+#pragma unroll
+                    for (int b = a; b < 6; ++b, ++k) hp[k] = __fma_rn(s[a], s[b], hp[k]);
+            }
+            col += r; row += q;
+            if (col >= dim) { col -= dim; ++row; }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 21; ++k) hp[k] = wsum(hp[k]);
+    if (H21 && lane < 21) {
+        double v = 0.0;
+#pragma unroll
+        for (int k = 0; k < 21; ++k)
+            if (k == lane) v = hp[k];
+        H21[(size_t)node * 21 + lane] = v;
+    }
+    if (lane == 0) {
+        double Hm[6][6], Hs[6][6];
+        for (int a = 0; a < 6; ++a)
+            for (int b = a; b < 6; ++b) {
+                Hm[a][b] = hp[tri21(a, b)];
+                Hm[b][a] = Hm[a][b];
+            }
+        const bool good = cond2x2_ok(Hm) && well_conditioned(Hm, half);
+        valid[node] = good ? 1 : 0;
+        ms[node] = make_float2(mean, sd);
+        // The step matrix of a whole-subset iteration (optimization_engine.cpp:
+        // 302-315): the LM-damped inverse when damping is on and the damped
+        // matrix is well conditioned, else the plain inverse.
+        bool done = false;
+        if (good && lm) {
+            double Hd[6][6];
+            for (int a = 0; a < 6; ++a)
+                for (int b = 0; b < 6; ++b) Hd[a][b] = Hm[a][b];
+            Hd[0][0] += (double)0.05f;
+            Hd[1][1] += (double)0.05f;
+            if (well_conditioned(Hd, half) && inverse6(Hd, Hs)) done = true;
+        }
+        if (good && !done && !inverse6(Hm, Hs)) valid[node] = 0;
+        double* o = Hs21 + (size_t)node * 21;
+        for (int a = 0; a < 6; ++a)
+            for (int b = a; b < 6; ++b) o[tri21(a, b)] = good ? Hs[a][b] : 0.0;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_image_prep(const uint8_t* px, const uint8_t* mask, int W, int H, float* I, float* gx,
+                              float* gy, cudaStream_t st) {
+    const int threads = 128;
+    const int per_row = (W + 3) / 4;
+    dim3 grid((per_row + threads - 1) / threads, H);
+    image_kernel<<<grid, threads, 0, st>>>(px, mask, W, H, I, gx, gy);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_grid_scan(const uint8_t* mask, int W, int H, int gridW, int gridH, int rect_x, int rect_y,
+                             int step, int dim, uint8_t* skip, int* n_valid, cudaStream_t st) {
+    const int nodes = gridW * gridH;
+    const int wpb = 8;
+    scan_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(mask, W, H, gridW, gridH, rect_x, rect_y, step, dim,
+                                                               skip, n_valid);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pool(const float* I, const float* gx, const float* gy, int W, int H, const uint8_t* skip,
+                        int gridW, int gridH, int rect_x, int rect_y, int step, int dim, int lm, uint8_t* valid,
+                        float2* ms, double* H21, double* Hs21, cudaStream_t st) {
+    const int nodes = gridW * gridH;
+    const int wpb = 4;
+    pool_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(I, gx, gy, W, H, skip, gridW, gridH, rect_x,
+                                                               rect_y, step, dim, lm, valid, ms, H21, Hs21);
+    return cudaGetLastError();
+}
+
+}  // namespace dic

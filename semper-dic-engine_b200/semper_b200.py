@@ -1,0 +1,362 @@
+"""Python binding of libsemper_c.so (ctypes) and of the speckle generator.
+
+The engine is the C ABI of include/semper_c.h; the stage entries are the
+kernel-level C ABI of include/semper_dic_cuda.h, here driven with torch device
+tensors. Nothing in this module computes on the CPU: a missing library, or a
+machine without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libsemper_c.so")
+SYNTH_PATH = os.path.join(HERE, "lib", "libsemper_synth.so")
+
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_vp = ctypes.c_void_p
+
+SEMPER_ERR_ROI, SEMPER_ERR_INIT, SEMPER_ERR_STRAIN_WINDOW, SEMPER_ERR_SEED, SEMPER_ERR_CANCELLED = -2, -3, -4, -5, -99
+INIT_AUTO_SEARCH, INIT_NO_SEARCH, INIT_NO_SIMPLEX = 0, 1, 2
+
+TASK_DT = np.dtype([("node", "<i4"), ("cx", "<i4"), ("cy", "<i4"), ("mode", "<i4"), ("g", "<f4", (6,))])
+RESULT_DT = np.dtype([("p", "<f4", (7,)), ("status", "<i4"), ("iters", "<i4"), ("trigger_iters", "<i4"),
+                      ("invalid_ref", "<i4"), ("flags", "<i4")])
+assert TASK_DT.itemsize == 40 and RESULT_DT.itemsize == 48
+
+C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_incremental_cancel",
+             "semper_incremental_create", "semper_incremental_destroy", "semper_incremental_init",
+             "semper_incremental_process", "semper_run", "semper_set_reference", "semper_version"]
+DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
+               "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
+               "dic_cuda_pack"]
+
+
+class SemperParams(ctypes.Structure):
+    _fields_ = [("rect_x", ctypes.c_int32), ("rect_y", ctypes.c_int32), ("rect_w", ctypes.c_int32),
+                ("rect_h", ctypes.c_int32), ("step", ctypes.c_int32), ("subset_size", ctypes.c_int32),
+                ("strain_window", ctypes.c_int32), ("use_6x6_interpolator", ctypes.c_int32)]
+
+
+class IncrementalInfo(ctypes.Structure):
+    _fields_ = [("reference_frame", ctypes.c_int32), ("reference_updated", ctypes.c_int32),
+                ("tracked_points", ctypes.c_int32), ("frame0_points", ctypes.c_int32),
+                ("taylor_fallbacks", ctypes.c_int32), ("lost_this_frame", ctypes.c_int32)]
+
+
+PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_void_p)
+
+_lib = None
+_synth = None
+
+
+def build() -> None:
+    """Compile the library in-tree (make; nvcc for sm_100a)."""
+    subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+
+
+def lib():
+    """The loaded libsemper_c.so (raises if it is absent and cannot be built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        L.semper_create.restype = _vp
+        L.semper_destroy.argtypes = [_vp]
+        L.semper_set_reference.argtypes = [_vp, _u8p, ctypes.c_size_t, _u8p, ctypes.c_size_t, ctypes.c_int,
+                                           ctypes.c_int]
+        L.semper_run.argtypes = [_vp, _u8p, ctypes.c_size_t, _u8p, ctypes.c_size_t, ctypes.POINTER(SemperParams),
+                                 _f32p, ctypes.c_int, _f32p, ctypes.c_int, PROGRESS_CB, _vp]
+        L.semper_cancel.argtypes = [_vp]
+        L.semper_version.restype = ctypes.c_char_p
+        L.semper_incremental_create.restype = _vp
+        L.semper_incremental_destroy.argtypes = [_vp]
+        L.semper_incremental_init.argtypes = [_vp, _u8p, ctypes.c_size_t, _u8p, ctypes.c_size_t, ctypes.c_int,
+                                              ctypes.c_int, ctypes.POINTER(SemperParams), ctypes.c_int32]
+        L.semper_incremental_process.argtypes = [_vp, _u8p, ctypes.c_size_t, _f32p, ctypes.c_int, _f32p,
+                                                 ctypes.c_int, ctypes.POINTER(IncrementalInfo), PROGRESS_CB, _vp]
+        L.semper_incremental_cancel.argtypes = [_vp]
+        L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 2 + [_vp] * 4
+        L.dic_cuda_grid_scan.argtypes = [_vp] + [ctypes.c_int] * 8 + [_vp, _vp, _vp]
+        L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 2 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
+        L.dic_cuda_solve.argtypes = [_vp] * 4 + [ctypes.c_int] * 2 + [_vp] * 3 + [ctypes.c_int] * 3 + \
+            [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]
+        L.dic_cuda_median_pass.argtypes = [ctypes.c_int] * 2 + [_vp] * 6
+        L.dic_cuda_clear_failed.argtypes = [ctypes.c_int, _vp, _vp, _vp]
+        L.dic_cuda_vsg.argtypes = [ctypes.c_int] * 4 + [_vp] * 7
+        L.dic_cuda_pack_scratch_bytes.argtypes = [ctypes.c_int]
+        L.dic_cuda_pack_scratch_bytes.restype = ctypes.c_size_t
+        L.dic_cuda_pack.argtypes = [ctypes.c_int] * 6 + [_vp] * 9 + [ctypes.c_size_t, _vp]
+        _lib = L
+    return _lib
+
+
+def synth_lib():
+    global _synth
+    if _synth is None:
+        if not os.path.exists(SYNTH_PATH):
+            build()
+        S = ctypes.CDLL(SYNTH_PATH)
+        S.synth_speckle.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_double,
+                                    ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                    ctypes.c_double, _f64p, ctypes.c_double, ctypes.c_uint64]
+        S.synth_speckle.restype = ctypes.c_int
+        S.synth_displacement.argtypes = [_f64p, ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+        _synth = S
+    return _synth
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+def params(rect, step, subset, window, six=False) -> SemperParams:
+    x, y, w, h = rect
+    return SemperParams(x, y, w, h, step, subset, window, 1 if six else 0)
+
+
+class Engine:
+    """semper_engine: one reference cache on the GPU (semper_create ...)."""
+
+    def __init__(self):
+        self._h = lib().semper_create()
+        if not self._h:
+            raise RuntimeError("semper_create failed (no usable CUDA device?)")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().semper_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def set_reference(self, gray: np.ndarray, mask: np.ndarray | None = None) -> int:
+        g = np.ascontiguousarray(gray, np.uint8)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        return lib().semper_set_reference(self._h, _p(g, _u8p), g.size, _p(m, _u8p), 0 if m is None else m.size,
+                                          g.shape[1], g.shape[0])
+
+    def run(self, deformed: np.ndarray, prm: SemperParams, capacity: int | None = None, mask=None,
+            metrics_len: int = 24, progress=None):
+        d = np.ascontiguousarray(deformed, np.uint8)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        if capacity is None:
+            capacity = max(prm.rect_w // max(prm.step, 1), 1) * max(prm.rect_h // max(prm.step, 1), 1) * 8
+        out = np.zeros(max(capacity, 1), np.float32)
+        met = np.zeros(max(metrics_len, 1), np.float32)
+        cb = PROGRESS_CB(progress) if progress else PROGRESS_CB()
+        rc = lib().semper_run(self._h, _p(d, _u8p), d.size, _p(m, _u8p), 0 if m is None else m.size,
+                              ctypes.byref(prm), _p(out, _f32p), capacity, _p(met, _f32p), metrics_len, cb, None)
+        return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy()
+
+    def cancel(self):
+        lib().semper_cancel(self._h)
+
+
+class Incremental:
+    """semper_incremental: a frame sequence against a moving reference."""
+
+    def __init__(self):
+        self._h = lib().semper_incremental_create()
+        if not self._h:
+            raise RuntimeError("semper_incremental_create failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().semper_incremental_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def init(self, ref, prm: SemperParams, update_interval: int, mask=None) -> int:
+        g = np.ascontiguousarray(ref, np.uint8)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        return lib().semper_incremental_init(self._h, _p(g, _u8p), g.size, _p(m, _u8p),
+                                             0 if m is None else m.size, g.shape[1], g.shape[0],
+                                             ctypes.byref(prm), update_interval)
+
+    def process(self, frame, capacity: int, metrics_len: int = 24):
+        d = np.ascontiguousarray(frame, np.uint8)
+        out = np.zeros(max(capacity, 1), np.float32)
+        met = np.zeros(max(metrics_len, 1), np.float32)
+        info = IncrementalInfo()
+        rc = lib().semper_incremental_process(self._h, _p(d, _u8p), d.size, _p(out, _f32p), capacity,
+                                              _p(met, _f32p), metrics_len, ctypes.byref(info), PROGRESS_CB(), None)
+        return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info
+
+
+def version() -> str:
+    return lib().semper_version().decode()
+
+
+# --------------------------------------------------------------- synthetic speckle
+def warp_block(cx=0.0, cy=0.0, u0=0.0, v0=0.0, a=(0.0, 0.0, 0.0, 0.0), su=0.0, Lu=0.0, sv=0.0, Lv=0.0,
+               modes=()) -> np.ndarray:
+    """The synth_speckle warp parameter block (see csrc/synth/speckle.cpp)."""
+    flat = [cx, cy, u0, v0, *a, su, Lu, sv, Lv, float(len(modes))]
+    for m in modes:
+        flat.extend(m)
+    return np.asarray(flat, np.float64)
+
+
+def speckle(w, h, seed, warp=None, noise=0.0, noise_seed=0, density=0.02, sigma=(1.5, 3.0), amp=(180.0, 220.0),
+            background=30.0) -> np.ndarray:
+    """One frame of the seeded Gaussian-blob speckle, optionally warped."""
+    out = np.zeros((h, w), np.uint8)
+    W = None if warp is None else np.ascontiguousarray(warp, np.float64)
+    rc = synth_lib().synth_speckle(_p(out, _u8p), w, h, seed, density, sigma[0], sigma[1], amp[0], amp[1],
+                                   background, _p(W, _f64p), noise, noise_seed)
+    if rc != 0:
+        raise RuntimeError("synth_speckle failed")
+    return out
+
+
+def displacement(warp, X, Y):
+    X = np.ascontiguousarray(X, np.float64).ravel()
+    Y = np.ascontiguousarray(Y, np.float64).ravel()
+    u = np.zeros_like(X)
+    v = np.zeros_like(X)
+    W = np.ascontiguousarray(warp, np.float64)
+    synth_lib().synth_displacement(_p(W, _f64p), X.size, _p(X, _f64p), _p(Y, _f64p), _p(u, _f64p), _p(v, _f64p))
+    return u, v
+
+
+def config_pair(cfg: int, size: int | None = None, pair: int = 0):
+    """(reference, deformed, params, warp) of a benchmark configuration.
+
+    cfg 0: 512^2, translation (0.4, -0.25), noise 1, step 10, subset 21, window 21.
+    cfg 1: 4096^2, u = 0.005 x + 2 sin(2 pi y / 256), v = -0.003 y + 1.5 sin(2 pi x / 384),
+           noise 2, step 4, subset 31, window 31.
+    cfg 4-plain: 4096^2 at the learned-seed comparison's solve settings (step 8,
+           subset 41, window 41) under the cfg-1 field (the large-motion warp
+           needs a global front end; see the proposal network).
+    `size` overrides the image edge (same field, same settings) for small cases.
+    """
+    if cfg == 0:
+        n = size or 512
+        warp = warp_block(u0=0.4, v0=-0.25)
+        prm = params((0, 0, n, n), 10, 21, 21)
+        noise = 1.0
+    elif cfg == 1:
+        n = size or 4096
+        warp = warp_block(a=(0.005, 0.0, 0.0, -0.003), su=2.0, Lu=256.0, sv=1.5, Lv=384.0)
+        prm = params((0, 0, n, n), 4, 31, 31)
+        noise = 2.0
+    elif cfg == 4:
+        n = size or 4096
+        warp = warp_block(a=(0.005, 0.0, 0.0, -0.003), su=2.0, Lu=256.0, sv=1.5, Lv=384.0)
+        prm = params((0, 0, n, n), 8, 41, 41)
+        noise = 2.0
+    else:
+        raise ValueError(cfg)
+    ref = speckle(n, n, 1000 + pair)
+    dfm = speckle(n, n, 1000 + pair, warp, noise, 2000 + 1)
+    return ref, dfm, prm, warp
+
+
+# --------------------------------------------------------------- kernel-level stages (torch device tensors)
+def _ptr(t):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+def _stream():
+    import torch
+
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ck(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"{what} failed with CUDA error {rc}")
+
+
+def image_prep(px, mask=None):
+    import torch
+
+    h, w = px.shape
+    I = torch.empty((h, w), dtype=torch.float32, device=px.device)
+    gx = torch.empty_like(I)
+    gy = torch.empty_like(I)
+    _ck(lib().dic_cuda_image_prep(_ptr(px), _ptr(mask), w, h, _ptr(I), _ptr(gx), _ptr(gy), _stream()), "image_prep")
+    return I, gx, gy
+
+
+def grid_scan(mask, w, h, grid, rect, step, subset):
+    import torch
+
+    gw, gh = grid
+    skip = torch.empty(gh * gw, dtype=torch.uint8, device="cuda")
+    nv = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _ck(lib().dic_cuda_grid_scan(_ptr(mask), w, h, gw, gh, rect[0], rect[1], step, subset, _ptr(skip), _ptr(nv),
+                                 _stream()), "grid_scan")
+    return skip, nv
+
+
+def hessian_pool(I, gx, gy, skip, grid, rect, step, subset, lm=True):
+    import torch
+
+    h, w = I.shape
+    gw, gh = grid
+    n = gw * gh
+    valid = torch.empty(n, dtype=torch.uint8, device="cuda")
+    ms = torch.empty((n, 2), dtype=torch.float32, device="cuda")
+    H = torch.empty((n, 21), dtype=torch.float64, device="cuda")
+    Hs = torch.empty((n, 21), dtype=torch.float64, device="cuda")
+    _ck(lib().dic_cuda_hessian_pool(_ptr(I), _ptr(gx), _ptr(gy), w, h, _ptr(skip), gw, gh, rect[0], rect[1], step,
+                                    subset, 1 if lm else 0, _ptr(valid), _ptr(ms), _ptr(H), _ptr(Hs), _stream()),
+        "hessian_pool")
+    return valid, ms, H, Hs
+
+
+def solve(ref_planes, def_I, pool, subset, tasks: np.ndarray, lm=True, six=False, blocks=0):
+    """tasks: TASK_DT array (node indexes into pool). Returns RESULT_DT array."""
+    import torch
+
+    rI, rgx, rgy = ref_planes
+    valid, ms, _H, Hs = pool
+    h, w = rI.shape
+    n = len(tasks)
+    tbytes = torch.from_numpy(np.ascontiguousarray(tasks).view(np.uint8).copy()).cuda()
+    res = torch.zeros(n * RESULT_DT.itemsize, dtype=torch.uint8, device="cuda")
+    q = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _ck(lib().dic_cuda_solve(_ptr(rI), _ptr(rgx), _ptr(rgy), _ptr(def_I), w, h, _ptr(valid), _ptr(ms), _ptr(Hs),
+                             subset, 1 if lm else 0, 1 if six else 0, _ptr(tbytes), n, _ptr(res), _ptr(q), blocks,
+                             _stream()), "solve")
+    torch.cuda.synchronize()
+    return res.cpu().numpy().view(RESULT_DT).copy()
+
+
+def median_vsg(u, v, valid, step, window):
+    """Median test (up to 5 passes) then VSG on device tensors; returns
+    (rejected, valid', exx, eyy, exy)."""
+    import torch
+
+    gh, gw = u.shape
+    ok = valid.clone()
+    fail = torch.zeros_like(ok)
+    nf = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rejected = 0
+    for _ in range(5):
+        nf.zero_()
+        _ck(lib().dic_cuda_median_pass(gw, gh, _ptr(u), _ptr(v), _ptr(ok), _ptr(fail), _ptr(nf), _stream()), "median")
+        k = int(nf.item())
+        if k == 0:
+            break
+        _ck(lib().dic_cuda_clear_failed(gw * gh, _ptr(ok), _ptr(fail), _stream()), "clear")
+        rejected += k
+    exx = torch.empty_like(u)
+    eyy = torch.empty_like(u)
+    exy = torch.empty_like(u)
+    _ck(lib().dic_cuda_vsg(gw, gh, step, window, _ptr(u), _ptr(v), _ptr(ok), _ptr(exx), _ptr(eyy), _ptr(exy),
+                           _stream()), "vsg")
+    torch.cuda.synchronize()
+    return rejected, ok, exx, eyy, exy
