@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the full-field DIC solve on B200: grid points per second.
+
+Workload (one "step" = one full-field solve of one deformed frame against a
+cached reference, i.e. frames 2+ of a fixed-reference batch): 4096 x 4096
+uint8 Gaussian-blob speckle (0.02 blobs/px^2, sigma U[1.5, 3], amplitude
+U[180, 220], background 30), deformed by u = 0.005 x + 2 sin(2 pi y / 256),
+v = -0.003 y + 1.5 sin(2 pi x / 384) with N(0, 2^2) noise; step 4, subset 31,
+strain window 31, 4x4 bicubic, whole image as ROI (1,048,576 grid nodes).
+
+  value     grid points written per second, inputs resident in HBM
+            (semper_b200_run_device), device time = CUDA events on the
+            engine's stream, max over ranks;
+  e2e       the same metric through the public C ABI (semper_run) with the
+            frame in pinned host memory: host->device frame copy and
+            device->host read of the packed points inside the timed region;
+  roofline  the IC-GN solve kernel (Path A launch): algorithmic FP32 FLOPs
+            (117 per subset pixel per iteration for the 4x4 kernel) over its
+            CUDA-event duration, against the FP32 CUDA-core peak;
+  cpu_baseline
+            the CPU restatement of the reference path (OpenMP, all host
+            threads) on a bounded ROI sample of the same frame pair.
+
+With --impl reference, rank 0 times that CPU implementation alone on the same
+metric and configuration (a bounded ROI sample per step) and prints its line.
+Multi-GPU (torchrun): every rank solves its own independent frame pair (its
+own speckle seed), no data-path collective; value = all ranks' points / the
+slowest rank's time ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "semper-dic-engine_b200"))
+
+FLOP_PER_PIXEL_ITER = {False: 117, True: 181}  # 4x4 bicubic / 6x6 Keys, per subset pixel per IC-GN iteration
+METRIC = "DIC grid points/sec on 1 B200 at <=0.01 px vs FP64; learned vs lattice seeding"
+WORKLOAD = ("cfg1: 4096x4096 uint8 speckle, u=0.005x+2sin(2pi y/256), v=-0.003y+1.5sin(2pi x/384), "
+            "noise sigma 2, step 4, subset 31, strain window 31, 4x4 bicubic, fixed reference (frames 2+)")
+
+
+def _env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def _peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def _ncu_traffic():
+    """DRAM bytes per launch of the IC-GN solve kernel from the committed ncu
+    summary (profiles/), scaled to one cfg1 launch; None if not recorded."""
+    p = os.path.join(REPO, "profiles", "icgn_solve_cfg1.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("traffic_bytes_per_cfg1_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip())
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.out = out
+        return False
+
+    def summary(self):
+        if self.proc is None or not getattr(self, "out", ""):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in csv.reader(io.StringIO(self.out)):
+            if len(row) < 9:
+                continue
+            try:
+                sm.append(float(row[1]))
+                smax.append(float(row[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, row[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(ref, dfm, prm, fp64=False):
+    """The CPU restatement on the central 1024 x 1024 ROI of the frame pair at
+    the same settings, reference cache warm (the solve timed is the second on
+    the reference). Returns (points, seconds, attempted)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+
+    n = ref.shape[0]
+    side = min(1024, n)
+    x0 = (n - side) // 2
+    p = [x0, x0, side, side, prm.step, prm.subset_size, prm.strain_window, prm.use_6x6_interpolator]
+    o = oracle.Oracle(fp64)
+    o.set_reference(ref)
+    o.run(dfm, p)  # frame 1: fills the grid scan + Hessian pool cache
+    t0 = time.perf_counter()
+    rc, pts, met = o.run(dfm, p)
+    dt = time.perf_counter() - t0
+    return rc, dt, int(met[0]), pts, p
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    import semper_b200 as sb
+
+    ref, dfm, prm, _ = sb.config_pair(1)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+
+    side = 1024
+    x0 = (ref.shape[0] - side) // 2
+    p = [x0, x0, side, side, prm.step, prm.subset_size, prm.strain_window, 0]
+    o = oracle.Oracle(False)
+    o.set_reference(ref)
+    for _ in range(max(args.warmup, 1)):
+        o.run(dfm, p)
+    pts_total, t_total = 0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rc, _, _ = o.run(dfm, p)
+        t_total += time.perf_counter() - t0
+        pts_total += rc
+    v = pts_total / t_total
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample": f"central {side}x{side} ROI of the 4096x4096 pair"},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
+                         "sample": f"central {side}x{side} ROI ({p[2] // p[4]}^2 grid) of the cfg1 pair, "
+                                   f"reference cache warm"},
+        "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    import semper_b200 as sb
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    ref, dfm, prm, warp = sb.config_pair(1, size=args.size, pair=rank)
+    H, W = ref.shape
+    grid_nodes = (prm.rect_w // prm.step) * (prm.rect_h // prm.step)
+    capacity = grid_nodes * 8
+
+    eng = sb.Engine()
+    assert eng.set_reference(ref) == 0
+    d_def = torch.from_numpy(dfm).cuda()
+    d_out = torch.empty(capacity, dtype=torch.float32, device="cuda")
+
+    # frame 1 on the reference: grid scan + Hessian pool built (reported apart)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    rc, met = eng.run_device(d_def, prm, d_out, capacity)
+    first_ms = 1000 * (time.perf_counter() - t0)
+    assert rc > 0, rc
+    first_t, _ = eng.last_timings()
+
+    for _ in range(args.warmup):
+        rc, met = eng.run_device(d_def, prm, d_out, capacity)
+
+    stream = torch.cuda.ExternalStream(eng.stream_handle())
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phases, counts = [], []
+    pts = 0
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            rc, met = eng.run_device(d_def, prm, d_out, capacity)
+            t, c = eng.last_timings()
+            phases.append(t)
+            counts.append(c)
+            pts += rc
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    pts_t = torch.tensor([pts], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(pts_t, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_t.item())
+    value = float(pts_t.item()) / args.steps / (ms_max / 1000.0)
+
+    # e2e: public C ABI, frame in pinned host memory, points read back
+    h_frame = torch.from_numpy(dfm).pin_memory()
+    frame_np = h_frame.numpy()
+    h_out = torch.empty(capacity, dtype=torch.float32).pin_memory().numpy()
+    e2e_ms = []
+    rc_e2e = 0
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        rc_e2e, _, _ = eng.run(frame_np, prm, capacity=capacity, out=h_out)
+        dt = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_ms.append(1000 * dt)
+    e2e_t = torch.tensor([statistics.mean(e2e_ms)], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = rc_e2e * world / (float(e2e_t.item()) / 1000.0)
+
+    # roofline of the IC-GN solve kernel (Path A launch)
+    a_ms = statistics.mean(p["path_a"] for p in phases)
+    a_pix = statistics.mean(c["path_a_pixel_iters"] for c in counts)
+    flops = FLOP_PER_PIXEL_ITER[bool(prm.use_6x6_interpolator)] * a_pix
+    achieved = flops / (a_ms / 1000.0) / 1e12
+    peaks, peak_src = _peaks()
+    sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
+    fp32_peak = sms * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
+    traffic = _ncu_traffic()
+    clocks = clk.summary()
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm)
+            cpu = {"value": crc / cdt, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
+                   "sample": f"central {cp[2]}x{cp[3]} ROI ({cp[2] // cp[4]}^2 grid, {catt} attempted) of the "
+                             f"same pair, reference cache warm, {cdt:.2f} s"}
+        mean_phase = {k: round(statistics.mean(p[k] for p in phases), 3) for k in phases[0]}
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD if args.size == 4096 else f"{WORKLOAD} [resized to {W}x{H}]",
+                       "image": [W, H], "grid_nodes": grid_nodes,
+                       "attempted": int(met[0]), "points_per_step": rc,
+                       "parallelism": f"replicas x{world} (independent frame pairs)",
+                       "l2": "inputs larger than L2: reference planes 201 MB + Hessian pool 177 MB + "
+                             "deformed plane 67 MB per step"},
+            "frames_per_s": 1000.0 / ms_max * world,
+            "attempted_points_per_s": int(met[0]) * world / (ms_max / 1000.0),
+            "first_frame_ms": round(first_ms, 2),
+            "first_frame_pool_ms": round(first_t["pool"], 3),
+            "phases_ms": mean_phase,
+            "mean_icgn_iters_per_point": float(met[8]),
+            "e2e": {"value": e2e_value, "unit": "points/s",
+                    "h2d_bytes_per_step": int(W * H), "d2h_bytes_per_step": int(rc_e2e * 32)},
+            "roofline": {"kernel": "icgn solve (Path A launch)", "bound": "fp32", "achieved": achieved,
+                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "traffic": traffic,
+                         "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 x {peaks.get('sm_max_mhz', 1965.0)} MHz "
+                                        f"({peak_src} sm_max_mhz)",
+                         "algorithmic": f"{FLOP_PER_PIXEL_ITER[False]} FLOP per subset pixel per iteration x "
+                                        f"{int(a_pix)} pixel-iterations per launch"},
+            "clocks": clocks,
+            "gpu_launches": int(sum(c["launches"] for c in counts)),
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--size", type=int, default=4096,
+                    help="image edge (default 4096, the benchmark workload; smaller sizes are for profiling)")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    local_rank = _env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank)
+    return run_b200(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -248,6 +248,10 @@ struct Engine::Impl {
     dic::MeshGrid mesh() { return dic::MeshGrid{gu.p, gv.p, gux.p, guy.p, gvx.p, gvy.p, in_mesh.p}; }
 
     void sync() { check(cudaStreamSynchronize(E.stream_), "stream sync"); }
+    void launched(int kernels, cudaError_t e, const char* what) {
+        check(e, what);
+        E.times_.launches += kernels;
+    }
     void poll_cancel() {
         if (E.h_cancel_[0]) throw Cancelled{};
     }
@@ -293,7 +297,7 @@ struct Engine::Impl {
         a.n_tasks_dev = nullptr;
         a.results = results.p;
         a.queue = counters.p;
-        check(dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)tk.size()), E.stream_), "solve");
+        launched(1, dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)tk.size()), E.stream_), "solve");
         check(cudaMemcpyAsync(out.data(), results.p, tk.size() * sizeof(dic_result), cudaMemcpyDeviceToHost,
                               E.stream_),
               "D2H results");
@@ -307,7 +311,7 @@ struct Engine::Impl {
         dI.ensure(n);
         dGx.ensure(n);
         dGy.ensure(n);
-        check(dic::launch_image_prep(d_def, nullptr, E.W_, E.H_, dI.p, dGx.p, dGy.p, E.stream_), "image prep");
+        launched(1, dic::launch_image_prep(d_def, nullptr, E.W_, E.H_, dI.p, dGx.p, dGy.p, E.stream_), "image prep");
     }
 
     int run(const uint8_t* d_def, const uint8_t* mask, Params params, float* d_out_p, int capacity,
@@ -460,7 +464,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 dm = dMask.p;
             }
             check(cudaMemsetAsync(counters.p + 2, 0, sizeof(int), st), "memset");
-            check(dic::launch_grid_scan(dm, W, H, gW, gH, params.rect_x, params.rect_y, params.step, dim, skip.p,
+            launched(1, dic::launch_grid_scan(dm, W, H, gW, gH, params.rect_x, params.rect_y, params.step, dim, skip.p,
                                         counters.p + 2, st),
                   "grid scan");
             int nv = 0;
@@ -470,7 +474,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             pool_valid.ensure(NG);
             pool_ms.ensure(NG);
             pool_Hs.ensure(NG * 21);
-            check(dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, skip.p, gW, gH, params.rect_x, params.rect_y,
+            launched(1, dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, skip.p, gW, gH, params.rect_x, params.rect_y,
                                    params.step, dim, 1, pool_valid.p, pool_ms.p, nullptr, pool_Hs.p, st),
                   "pool");
             h_skip.resize(NG);
@@ -496,7 +500,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         gtmp.ensure(NG); in_mesh.ensure(NG);
         check(cudaMemcpyAsync(fsolved.p, skip.p, NG, cudaMemcpyDeviceToDevice, st), "init solved");
         check(cudaMemsetAsync(ftag.p, 0, NG, st), "init tag");
-        check(dic::launch_fill(fcorr.p, (int)NG, -1.0f, st), "init corr");
+        launched(1, dic::launch_fill(fcorr.p, (int)NG, -1.0f, st), "init corr");
         std::vector<uint8_t> solved = h_skip;  // host mirror of the solved flags
         const int total = total_valid;
 
@@ -695,7 +699,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 check(cudaMemcpyAsync(scat.p, recs.data(), recs.size() * sizeof(dic::ScatterRec),
                                       cudaMemcpyHostToDevice, st),
                       "H2D anchors");
-                check(dic::launch_scatter((int)recs.size(), scat.p, field(), st), "scatter anchors");
+                launched(1, dic::launch_scatter((int)recs.size(), scat.p, field(), st), "scatter anchors");
                 check(cudaMemsetAsync(ftag.p, 0, NG, st), "tag");
             }
         }
@@ -709,7 +713,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
 
         // ---------------------------------------------------------------- mesh guesses
         const auto t_mesh = clk::now();
-        check(dic::launch_init_guess((int)NG, globalU, globalV, mesh(), st), "init guess");
+        launched(1, dic::launch_init_guess((int)NG, globalU, globalV, mesh(), st), "init guess");
         std::vector<dic::MeshTri> htris;
         {
             std::vector<semper_geom::Pt> ins;
@@ -756,11 +760,11 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         const bool use_h = homography.size() == 9;
         if (use_h)
             for (int k = 0; k < 9; ++k) hg.h[k] = homography[k];
-        check(dic::launch_mesh_assign(gW, gH, params.rect_x, params.rect_y, params.step, tris.p, (int)htris.size(),
+        launched((htris.empty() ? 0 : (quality == Quality::FULL ? 2 : 1)) + (use_h ? 1 : 0), dic::launch_mesh_assign(gW, gH, params.rect_x, params.rect_y, params.step, tris.p, (int)htris.size(),
                                       quality == Quality::FULL ? 1 : 0, use_h ? &hg : nullptr, fsolved.p, ftag.p,
                                       mesh(), st),
               "mesh assign");
-        check(dic::launch_smooth(gW, gH, params.step, mesh(), gtmp.p, st), "smooth");
+        launched(6, dic::launch_smooth(gW, gH, params.step, mesh(), gtmp.p, st), "smooth");
         check(cudaEventRecord(ev[4], st), "event");
         sync();
         const double ms_mesh = ms_since(t_mesh);
@@ -841,7 +845,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         results.ensure(std::max(results.n, NG));
         check(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st), "counters");
         check(cudaMemsetAsync(pstats.p, 0, sizeof(dic::PathStats), st), "stats");
-        check(dic::launch_path_a_tasks(gW, gH, params.rect_x, params.rect_y, params.step, fsolved.p, ftag.p, mesh(),
+        launched(1, dic::launch_path_a_tasks(gW, gH, params.rect_x, params.rect_y, params.step, fsolved.p, ftag.p, mesh(),
                                        tasks.p, counters.p + 1, st),
               "path A tasks");
         int n_a = 0;
@@ -855,9 +859,9 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             a.results = results.p;
             a.queue = counters.p;
             check(cudaEventRecord(ev[5], st), "event");
-            check(dic::launch_solve(a, params.six ? 1 : 0, solve_grid(n_a), st), "path A solve");
+            launched(1, dic::launch_solve(a, params.six ? 1 : 0, solve_grid(n_a), st), "path A solve");
             check(cudaEventRecord(ev[6], st), "event");
-            check(dic::launch_commit(tasks.p, counters.p + 1, n_a, results.p, field(), pstats.p, st), "path A commit");
+            launched(1, dic::launch_commit(tasks.p, counters.p + 1, n_a, results.p, field(), pstats.p, st), "path A commit");
         }
         dic::PathStats ps{};
         check(cudaMemcpyAsync(&ps, pstats.p, sizeof(ps), cudaMemcpyDeviceToHost, st), "D2H stats");
@@ -874,6 +878,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         st_a.simp_calls = ps.simp_calls;
         st_a.simp_saved = ps.simp_saved;
         st_a.simp_dead = ps.simp_dead;
+        E.times_.path_a_pixel_iters = (long long)dim * dim * st_a.icgn_iters;
         const double ms_a = ms_since(t_a);
         ticker.set(90);
 
@@ -883,7 +888,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             check(cudaMemcpyAsync(solved.data(), fsolved.p, NG, cudaMemcpyDeviceToHost, st), "D2H solved");
             bseeds.ensure(std::max<size_t>(bseeds.n, NG));
             check(cudaMemsetAsync(counters.p + 7, 0, sizeof(int), st), "memset");
-            check(dic::launch_boundary(gW, gH, field(), bseeds.p, counters.p + 7, st), "boundary");
+            launched(1, dic::launch_boundary(gW, gH, field(), bseeds.p, counters.p + 7, st), "boundary");
             int nb = 0;
             check(cudaMemcpyAsync(&nb, counters.p + 7, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H nb");
             sync();
@@ -1035,7 +1040,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 check(cudaMemcpyAsync(scat.p, recs.data(), recs.size() * sizeof(dic::ScatterRec),
                                       cudaMemcpyHostToDevice, st),
                       "H2D path B");
-                check(dic::launch_scatter((int)recs.size(), scat.p, field(), st), "scatter path B");
+                launched(1, dic::launch_scatter((int)recs.size(), scat.p, field(), st), "scatter path B");
             }
         }
         check(cudaEventRecord(ev[7], st), "event");
@@ -1060,25 +1065,25 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         // ---------------------------------------------------------------- pack + strain
         const auto t_strain = clk::now();
         valid.ensure(NG); fail.ensure(NG); exx.ensure(NG); eyy.ensure(NG); exy.ensure(NG);
-        check(dic::launch_valid((int)NG, field(), valid.p, st), "valid");
+        launched(1, dic::launch_valid((int)NG, field(), valid.p, st), "valid");
         int dropped_outlier = 0;
         for (int pass = 0; pass < 5; ++pass) {
             check(cudaMemsetAsync(counters.p + 3, 0, sizeof(int), st), "memset");
-            check(dic::launch_median_pass(gW, gH, fu.p, fv.p, valid.p, fail.p, counters.p + 3, st), "median");
+            launched(1, dic::launch_median_pass(gW, gH, fu.p, fv.p, valid.p, fail.p, counters.p + 3, st), "median");
             int nf = 0;
             check(cudaMemcpyAsync(&nf, counters.p + 3, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H fail");
             sync();
             if (nf == 0) break;
-            check(dic::launch_clear_failed((int)NG, valid.p, fail.p, st), "clear");
+            launched(1, dic::launch_clear_failed((int)NG, valid.p, fail.p, st), "clear");
             dropped_outlier += nf;
         }
-        check(dic::launch_vsg(gW, gH, params.step, params.strain_window, fu.p, fv.p, valid.p, exx.p, eyy.p, exy.p, st),
+        launched(1, dic::launch_vsg(gW, gH, params.step, params.strain_window, fu.p, fv.p, valid.p, exx.p, eyy.p, exy.p, st),
               "vsg");
         const size_t scr = dic::pack_scratch_bytes((int)NG);
         pack_scratch.ensure(std::max(pack_scratch.n, scr));
         check(cudaMemsetAsync(counters.p + 4, 0, 3 * sizeof(int), st), "memset");
         const int max_pts = capacity / 8;
-        check(dic::launch_pack(gW, gH, params.rect_x, params.rect_y, params.step, max_pts, valid.p, fu.p, fv.p,
+        launched(4, dic::launch_pack(gW, gH, params.rect_x, params.rect_y, params.step, max_pts, valid.p, fu.p, fv.p,
                                fcorr.p, exx.p, eyy.p, exy.p, d_out_p, counters.p + 4, counters.p + 5, pack_scratch.p,
                                pack_scratch.n, st),
               "pack");

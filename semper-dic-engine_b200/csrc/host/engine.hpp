@@ -73,6 +73,8 @@ struct PhaseTimes {
     long long icgn_iters = 0;   // IC-GN iterations of every subset solve
     long long pixel_iters = 0;  // subset pixels x iterations (the IC-GN work)
     int path_a_tasks = 0;
+    long long path_a_pixel_iters = 0;  // the same for the Path A launch alone
+    int launches = 0;                  // kernels this library launched during the solve
 };
 
 class Engine {

@@ -11,6 +11,7 @@
 #include <memory>
 #include <vector>
 
+#include "../../../include/semper_b200_ext.h"
 #include "../../../include/semper_c.h"
 #include "engine.hpp"
 #include "incremental.hpp"
@@ -99,6 +100,8 @@ struct semper_engine {
     Engine engine;
     CancelWindow window;
     std::atomic<bool> busy{false};
+    bool has_model = false;
+    double model[9] = {};
 };
 
 struct semper_incremental {
@@ -168,14 +171,18 @@ SEMPER_C_API int semper_run(semper_engine* eng, const uint8_t* def, size_t def_l
         if (!eng->engine.has_reference()) return SEMPER_ERR_INIT;
         const int w = eng->engine.width(), h = eng->engine.height();
         std::vector<uint8_t> d, m;
-        if (!decode_raw(def, def_len, w, h, d)) return SEMPER_ERR_INIT;
+        const uint8_t* frame = def;  // a raw 8-bit frame is used in place
+        if ((uint64_t)def_len != (uint64_t)w * (uint64_t)h) {
+            if (!decode_raw(def, def_len, w, h, d)) return SEMPER_ERR_INIT;
+            frame = d.data();
+        }
         bool has_mask = false;
         if (!decode_mask(mask, mask_len, w, h, m, has_mask)) return SEMPER_ERR_INIT;
         semper_b200::Progress progress;
         if (cb) progress = [cb, user](int pct) { cb(pct, user); };
         window_enter(eng->engine, eng->window);
-        return eng->engine.run(d.data(), has_mask ? m.data() : nullptr, to_params(params), out, out_capacity,
-                               metrics, metrics_len, nullptr, progress);
+        return eng->engine.run(frame, has_mask ? m.data() : nullptr, to_params(params), out, out_capacity,
+                               metrics, metrics_len, eng->has_model ? eng->model : nullptr, progress);
     });
 }
 
@@ -184,6 +191,52 @@ SEMPER_C_API void semper_cancel(semper_engine* eng) {
 }
 
 SEMPER_C_API const char* semper_version(void) { return "0.6.1"; }
+
+SEMPER_C_API int semper_b200_run_device(semper_engine* eng, const uint8_t* d_def, const semper_params* params,
+                                        float* d_out, int out_capacity, float* metrics, int metrics_len) {
+    if (eng == nullptr || d_def == nullptr || params == nullptr || d_out == nullptr || out_capacity < 0)
+        return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        WindowScope scope(eng->engine, eng->window);
+        if (!eng->engine.has_reference()) return SEMPER_ERR_INIT;
+        window_enter(eng->engine, eng->window);
+        return eng->engine.run_device(d_def, nullptr, to_params(params), d_out, out_capacity, metrics, metrics_len,
+                                      eng->has_model ? eng->model : nullptr);
+    });
+}
+
+SEMPER_C_API void* semper_b200_stream(semper_engine* eng) {
+    return eng ? (void*)eng->engine.stream() : nullptr;
+}
+
+SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], long long counts[5]) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    const semper_b200::PhaseTimes& t = eng->engine.last_times();
+    if (times) {
+        const float v[8] = {t.prep, t.pool, t.seed, t.mesh, t.path_a, t.path_b, t.strain, t.total};
+        for (int i = 0; i < 8; ++i) times[i] = v[i];
+    }
+    if (counts) {
+        counts[0] = t.icgn_iters;
+        counts[1] = t.pixel_iters;
+        counts[2] = t.path_a_tasks;
+        counts[3] = t.path_a_pixel_iters;
+        counts[4] = t.launches;
+    }
+    return 0;
+}
+
+SEMPER_C_API int semper_b200_set_global_model(semper_engine* eng, const double* h9) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    eng->has_model = h9 != nullptr;
+    if (h9)
+        for (int i = 0; i < 9; ++i) eng->model[i] = h9[i];
+    return 0;
+}
 
 SEMPER_C_API semper_incremental* semper_incremental_create(void) {
     return guarded<semper_incremental*>(nullptr, [] {

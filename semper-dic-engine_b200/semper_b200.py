@@ -35,6 +35,8 @@ assert TASK_DT.itemsize == 40 and RESULT_DT.itemsize == 48
 C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_incremental_cancel",
              "semper_incremental_create", "semper_incremental_destroy", "semper_incremental_init",
              "semper_incremental_process", "semper_run", "semper_set_reference", "semper_version"]
+EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
+               "semper_b200_stream"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
                "dic_cuda_pack"]
@@ -85,6 +87,12 @@ def lib():
         L.semper_incremental_process.argtypes = [_vp, _u8p, ctypes.c_size_t, _f32p, ctypes.c_int, _f32p,
                                                  ctypes.c_int, ctypes.POINTER(IncrementalInfo), PROGRESS_CB, _vp]
         L.semper_incremental_cancel.argtypes = [_vp]
+        L.semper_b200_run_device.argtypes = [_vp, _vp, ctypes.POINTER(SemperParams), _vp, ctypes.c_int, _f32p,
+                                             ctypes.c_int]
+        L.semper_b200_stream.argtypes = [_vp]
+        L.semper_b200_stream.restype = _vp
+        L.semper_b200_last_timings.argtypes = [_vp, _f32p, ctypes.POINTER(ctypes.c_longlong)]
+        L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
         L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 2 + [_vp] * 4
         L.dic_cuda_grid_scan.argtypes = [_vp] + [ctypes.c_int] * 8 + [_vp, _vp, _vp]
         L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 2 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
@@ -146,12 +154,15 @@ class Engine:
                                           g.shape[1], g.shape[0])
 
     def run(self, deformed: np.ndarray, prm: SemperParams, capacity: int | None = None, mask=None,
-            metrics_len: int = 24, progress=None):
+            metrics_len: int = 24, progress=None, out: np.ndarray | None = None):
+        """semper_run. `out` (float32, >= capacity) may be a caller buffer,
+        e.g. pinned memory; the returned points are a copy either way."""
         d = np.ascontiguousarray(deformed, np.uint8)
         m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
         if capacity is None:
             capacity = max(prm.rect_w // max(prm.step, 1), 1) * max(prm.rect_h // max(prm.step, 1), 1) * 8
-        out = np.zeros(max(capacity, 1), np.float32)
+        if out is None:
+            out = np.zeros(max(capacity, 1), np.float32)
         met = np.zeros(max(metrics_len, 1), np.float32)
         cb = PROGRESS_CB(progress) if progress else PROGRESS_CB()
         rc = lib().semper_run(self._h, _p(d, _u8p), d.size, _p(m, _u8p), 0 if m is None else m.size,
@@ -160,6 +171,28 @@ class Engine:
 
     def cancel(self):
         lib().semper_cancel(self._h)
+
+    def run_device(self, d_def, prm: SemperParams, d_out, capacity: int, metrics_len: int = 24):
+        """semper_b200_run_device: deformed frame and output are device tensors."""
+        met = np.zeros(max(metrics_len, 1), np.float32)
+        rc = lib().semper_b200_run_device(self._h, ctypes.c_void_p(d_def.data_ptr()), ctypes.byref(prm),
+                                          ctypes.c_void_p(d_out.data_ptr()), capacity, _p(met, _f32p), metrics_len)
+        return rc, met[:metrics_len].copy()
+
+    def stream_handle(self) -> int:
+        return lib().semper_b200_stream(self._h) or 0
+
+    def last_timings(self):
+        t = np.zeros(8, np.float32)
+        c = (ctypes.c_longlong * 5)()
+        lib().semper_b200_last_timings(self._h, _p(t, _f32p), c)
+        names = ["prep", "pool", "seed", "mesh", "path_a", "path_b", "strain", "total"]
+        counts = ["icgn_iters", "pixel_iters", "path_a_tasks", "path_a_pixel_iters", "launches"]
+        return dict(zip(names, map(float, t))), dict(zip(counts, map(int, c)))
+
+    def set_global_model(self, H=None) -> int:
+        Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
+        return lib().semper_b200_set_global_model(self._h, _p(Hm, _f64p))
 
 
 class Incremental:

@@ -24,8 +24,10 @@ def test_library_exports_exactly_the_declared_symbols():
     exported = sorted(line.split()[-1] for line in out.stdout.splitlines() if line.strip())
     c_api = _declared("semper_c.h", r"\b(semper_[a-z_]+)\s*\(")
     dic_api = _declared("semper_dic_cuda.h", r"\b(dic_cuda_[a-z0-9_]+)\s*\(")
+    ext_api = _declared("semper_b200_ext.h", r"\b(semper_b200_[a-z0-9_]+)\s*\(")
     assert c_api == sorted(sb.C_SYMBOLS)
-    assert exported == sorted(c_api + dic_api)
+    assert ext_api == sorted(sb.EXT_SYMBOLS)
+    assert exported == sorted(c_api + dic_api + ext_api)
     for name in exported:
         assert hasattr(lib, name)
 
