@@ -6,7 +6,9 @@
  * do, against the CPU restatement) and embedded in other pipelines.
  *
  * Conventions: every pointer named d_* is device memory; images are
- * row-major, width-fastest; `stream` is a cudaStream_t (NULL = default
+ * row-major, width-fastest; float planes have a row pitch (elements) that is
+ * a multiple of 4 (16-byte rows, which the TMA tile loads need), input bytes
+ * are tight (pitch = width); `stream` is a cudaStream_t (NULL = default
  * stream). Each call enqueues work and returns 0, or a cudaError_t value if a
  * launch failed. Nothing here allocates or synchronises unless stated.
  */
@@ -26,7 +28,7 @@ extern "C" {
    and, with d_mask, stamp_ghost_wall (src/pipeline/reference_cache.cpp:18-35):
    u8 -> f32 intensity, 4th-order central-difference gradients, -10 where the
    mask is below 128. */
-int dic_cuda_image_prep(const uint8_t* d_px, const uint8_t* d_mask, int width, int height,
+int dic_cuda_image_prep(const uint8_t* d_px, const uint8_t* d_mask, int width, int height, int pitch,
                         float* d_I, float* d_gx, float* d_gy, void* stream);
 
 /* The grid validity scan of run_full_field_impl
@@ -43,7 +45,7 @@ int dic_cuda_grid_scan(const uint8_t* d_mask, int width, int height, int grid_w,
    flag, (mean, std) as two floats, the Hessian and the step matrix as 21
    doubles each (upper triangle, row-major; d_H21 may be NULL). */
 int dic_cuda_hessian_pool(const float* d_I, const float* d_gx, const float* d_gy, int width, int height,
-                          const uint8_t* d_skip, int grid_w, int grid_h, int rect_x, int rect_y, int step,
+                          int pitch, const uint8_t* d_skip, int grid_w, int grid_h, int rect_x, int rect_y, int step,
                           int subset, int lm, uint8_t* d_valid, float* d_mean_std, double* d_H21,
                           double* d_Hs21, void* stream);
 
@@ -55,7 +57,7 @@ int dic_cuda_hessian_pool(const float* d_I, const float* d_gx, const float* d_gy
    dic_task.node. d_queue is a work counter that must be zero at launch.
    `blocks` = persistent grid size (0 = one wave). */
 int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const float* d_ref_gy, const float* d_def_I,
-                   int width, int height, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
+                   int width, int height, int pitch, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
                    const double* d_pool_Hs21, int subset, int lm, int six, const dic_task* d_tasks, int n_tasks,
                    dic_result* d_results, int* d_queue, int blocks, void* stream);
 

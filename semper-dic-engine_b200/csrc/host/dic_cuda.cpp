@@ -14,9 +14,9 @@ namespace {
 cudaStream_t S(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 }
 
-DIC_API int dic_cuda_image_prep(const uint8_t* d_px, const uint8_t* d_mask, int width, int height, float* d_I,
-                                float* d_gx, float* d_gy, void* stream) {
-    return (int)dic::launch_image_prep(d_px, d_mask, width, height, d_I, d_gx, d_gy, S(stream));
+DIC_API int dic_cuda_image_prep(const uint8_t* d_px, const uint8_t* d_mask, int width, int height, int pitch,
+                                float* d_I, float* d_gx, float* d_gy, void* stream) {
+    return (int)dic::launch_image_prep(d_px, d_mask, width, height, pitch, d_I, d_gx, d_gy, S(stream));
 }
 
 DIC_API int dic_cuda_grid_scan(const uint8_t* d_mask, int width, int height, int grid_w, int grid_h, int rect_x,
@@ -26,15 +26,15 @@ DIC_API int dic_cuda_grid_scan(const uint8_t* d_mask, int width, int height, int
 }
 
 DIC_API int dic_cuda_hessian_pool(const float* d_I, const float* d_gx, const float* d_gy, int width, int height,
-                                  const uint8_t* d_skip, int grid_w, int grid_h, int rect_x, int rect_y, int step,
+                                  int pitch, const uint8_t* d_skip, int grid_w, int grid_h, int rect_x, int rect_y, int step,
                                   int subset, int lm, uint8_t* d_valid, float* d_mean_std, double* d_H21,
                                   double* d_Hs21, void* stream) {
-    return (int)dic::launch_pool(d_I, d_gx, d_gy, width, height, d_skip, grid_w, grid_h, rect_x, rect_y, step, subset,
+    return (int)dic::launch_pool(d_I, d_gx, d_gy, width, height, pitch, d_skip, grid_w, grid_h, rect_x, rect_y, step, subset,
                                  lm, d_valid, reinterpret_cast<float2*>(d_mean_std), d_H21, d_Hs21, S(stream));
 }
 
 DIC_API int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const float* d_ref_gy, const float* d_def_I,
-                           int width, int height, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
+                           int width, int height, int pitch, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
                            const double* d_pool_Hs21, int subset, int lm, int six, const dic_task* d_tasks,
                            int n_tasks, dic_result* d_results, int* d_queue, int blocks, void* stream) {
     if (n_tasks <= 0) return 0;
@@ -45,6 +45,8 @@ DIC_API int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const fl
     a.defI = d_def_I;
     a.W = width;
     a.H = height;
+    a.pitch = pitch;
+    a.err = nullptr;
     a.pool_valid = d_pool_valid;
     a.pool_ms = reinterpret_cast<const float2*>(d_pool_mean_std);
     a.pool_Hs = d_pool_Hs21;

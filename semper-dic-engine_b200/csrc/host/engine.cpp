@@ -264,6 +264,8 @@ struct Engine::Impl {
         a.defI = dI.p;
         a.W = E.W_;
         a.H = E.H_;
+        a.pitch = pitch();
+        a.err = counters.p + 9;
         a.pool_valid = pool_valid.p;
         a.pool_ms = pool_ms.p;
         a.pool_Hs = pool_Hs.p;
@@ -306,12 +308,15 @@ struct Engine::Impl {
         return out;
     }
 
+    int pitch() const { return (E.W_ + 3) & ~3; }
+
     void prepare_deformed(const uint8_t* d_def) {
-        const size_t n = (size_t)E.W_ * E.H_;
+        const size_t n = (size_t)pitch() * E.H_;
         dI.ensure(n);
         dGx.ensure(n);
         dGy.ensure(n);
-        launched(1, dic::launch_image_prep(d_def, nullptr, E.W_, E.H_, dI.p, dGx.p, dGy.p, E.stream_), "image prep");
+        launched(1, dic::launch_image_prep(d_def, nullptr, E.W_, E.H_, pitch(), dI.p, dGx.p, dGy.p, E.stream_),
+                 "image prep");
     }
 
     int run(const uint8_t* d_def, const uint8_t* mask, Params params, float* d_out_p, int capacity,
@@ -352,11 +357,12 @@ int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask
     if (!gray || w <= 0 || h <= 0) return -3;
     if ((int64_t)w * h > (int64_t)INT32_MAX) return -3;
     const size_t n = (size_t)w * h;
+    const size_t np = (size_t)((w + 3) & ~3) * h;  // planes: rows padded to 16 bytes (TMA)
     Impl& I = *impl_;
     I.dGray.ensure(n);
-    I.rI.ensure(n);
-    I.rGx.ensure(n);
-    I.rGy.ensure(n);
+    I.rI.ensure(np);
+    I.rGx.ensure(np);
+    I.rGy.ensure(np);
     check(cudaMemcpyAsync(I.dGray.p, gray, n, cudaMemcpyHostToDevice, stream_), "H2D reference");
     const uint8_t* dm = nullptr;
     if (mask) {
@@ -364,7 +370,8 @@ int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask
         check(cudaMemcpyAsync(I.dMask.p, mask, n, cudaMemcpyHostToDevice, stream_), "H2D mask");
         dm = I.dMask.p;
     }
-    check(dic::launch_image_prep(I.dGray.p, dm, w, h, I.rI.p, I.rGx.p, I.rGy.p, stream_), "reference prep");
+    check(dic::launch_image_prep(I.dGray.p, dm, w, h, (w + 3) & ~3, I.rI.p, I.rGx.p, I.rGy.p, stream_),
+          "reference prep");
     check(cudaStreamSynchronize(stream_), "reference sync");
     W_ = w;
     H_ = h;
@@ -385,14 +392,14 @@ int Engine::adopt_last_deformed(const uint8_t* mask) {
     if (mask) {
         // Ghost Wall on the adopted frame: the gradients stay those of the
         // real intensities (stamp after prepare, reference_cache.cpp:95-96).
-        const size_t n = (size_t)W_ * H_;
-        I.dMask.ensure(n);
-        check(cudaMemcpyAsync(I.dMask.p, mask, n, cudaMemcpyHostToDevice, stream_), "H2D mask");
+        const int P = (W_ + 3) & ~3;
+        const size_t n = (size_t)P * H_;
         std::vector<float> plane(n);
         check(cudaMemcpyAsync(plane.data(), I.rI.p, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H plane");
         check(cudaStreamSynchronize(stream_), "sync");
-        for (size_t k = 0; k < n; ++k)
-            if (mask[k] < 128) plane[k] = -10.0f;
+        for (int y = 0; y < H_; ++y)
+            for (int x = 0; x < W_; ++x)
+                if (mask[(size_t)y * W_ + x] < 128) plane[(size_t)y * P + x] = -10.0f;
         check(cudaMemcpyAsync(I.rI.p, plane.data(), n * 4, cudaMemcpyHostToDevice, stream_), "H2D plane");
         check(cudaStreamSynchronize(stream_), "sync");
     }
@@ -474,7 +481,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             pool_valid.ensure(NG);
             pool_ms.ensure(NG);
             pool_Hs.ensure(NG * 21);
-            launched(1, dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, skip.p, gW, gH, params.rect_x, params.rect_y,
+            launched(1, dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, pitch(), skip.p, gW, gH, params.rect_x, params.rect_y,
                                    params.step, dim, 1, pool_valid.p, pool_ms.p, nullptr, pool_Hs.p, st),
                   "pool");
             h_skip.resize(NG);

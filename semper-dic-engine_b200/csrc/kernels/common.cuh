@@ -108,6 +108,42 @@ __device__ __forceinline__ float interp6(const float* __restrict__ base, int pit
     return val;
 }
 
+// The same from a shared-memory tile (row pitch `pitch`), same arithmetic.
+__device__ __forceinline__ float interp4s(const float* base, int pitch, int xi, int yi, float dx, float dy) {
+    float wx[4], wy[4];
+    cubic_weights(dx, wx);
+    cubic_weights(dy, wy);
+    const float* r = base + (yi - 1) * pitch + (xi - 1);
+    float val = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float* q = r + j * pitch;
+        float rv = q[0] * wx[0];
+        rv = __fmaf_rn(q[1], wx[1], rv);
+        rv = __fmaf_rn(q[2], wx[2], rv);
+        rv = __fmaf_rn(q[3], wx[3], rv);
+        val = (j == 0) ? rv * wy[0] : __fmaf_rn(rv, wy[j], val);
+    }
+    return val;
+}
+
+__device__ __forceinline__ float interp6s(const float* base, int pitch, int xi, int yi, float dx, float dy) {
+    float wx[6], wy[6];
+    keys6_weights(dx, wx);
+    keys6_weights(dy, wy);
+    const float* r = base + (yi - 2) * pitch + (xi - 2);
+    float val = 0.0f;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        const float* q = r + j * pitch;
+        float rv = q[0] * wx[0];
+#pragma unroll
+        for (int i = 1; i < 6; ++i) rv = __fmaf_rn(q[i], wx[i], rv);
+        val = (j == 0) ? rv * wy[0] : __fmaf_rn(rv, wy[j], val);
+    }
+    return val;
+}
+
 // The 6x6 FP64 helpers of the Hessian: Cholesky, explicit inverse, and the
 // scaled 1-norm reciprocal condition (src/math/hessian.hpp:40-52).
 static __device__ __noinline__ bool cholesky6(const double A[6][6], double L[6][6]) {

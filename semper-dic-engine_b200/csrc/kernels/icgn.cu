@@ -6,14 +6,23 @@
 // solve_icgn (:272-465) / solve_simplex (:531-651) / estimate_initial_guess
 // (:120-179), then reject_if_ghosted (src/pipeline/full_field_internal.hpp:347-353).
 //
-// Layout per warp (dynamic shared memory): the FP64 step matrices, the
-// sampled deformed values and their validity for the subset's n pixels.
-// Pixel i of the subset (row-major) belongs to lane i % 32.
+// Layout per warp (dynamic shared memory, 128-byte aligned): an mbarrier, the
+// FP64 step matrices, a tile of the deformed image staged by 2-D TMA around
+// the warped subset, and the subset's sampled values, their validity and its
+// reference (non-Ghost-Wall) flags. Pixel i of the subset (row-major) belongs
+// to lane i % 32. Samples whose 4x4 / 6x6 support lies in the tile read shared
+// memory; any other sample reads the image through the read-only cache, with
+// the same arithmetic, so the tile only ever changes where the values come from.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 #include "dic_types.h"
 #include "icgn.cuh"
+#include "tma.cuh"
+
+#include <cstring>
 
 namespace dic {
 
@@ -54,18 +63,90 @@ struct WarpSolver {
     float mref, iref;
     int min_valid;
     size_t ref_base;  // index of the subset's top-left pixel in the planes
+    uint64_t* bar;    // TMA completion barrier
     double* Href;     // [36] step matrix of a whole-subset iteration
     double* Hmask;    // [36] step matrix of a masked iteration
+    float* tile;      // [tile_h][tile_w] deformed-image tile
     float* vals;      // [n]
     uint8_t* valid;   // [n]
+    uint8_t* refok;   // [n] reference pixel outside the Ghost Wall
     int simplex_runs;
+    const CUtensorMap* tmap;
+    int tx0, ty0;         // tile origin, image pixels
+    bool tile_ok;         // the tile holds the box at (tx0, ty0)
+    bool tile_on;         // TMA staging enabled for this warp
+    uint32_t phase;       // parity of the next barrier phase
 
-    __device__ WarpSolver(const SolveArgs& args, int ln, unsigned char* sm) : a(args), lane(ln) {
-        Href = reinterpret_cast<double*>(sm);
+    __device__ WarpSolver(const SolveArgs& args, int ln, unsigned char* sm, const CUtensorMap* map,
+                          uint32_t ph)
+        : a(args), lane(ln), tmap(map), phase(ph) {
+        const SmemLayout L = smem_layout(a.max_n, a.tile_w, a.tile_h);
+        bar = reinterpret_cast<uint64_t*>(sm);
+        Href = reinterpret_cast<double*>(sm + L.off_h);
         Hmask = Href + 36;
-        vals = reinterpret_cast<float*>(Hmask + 36);
-        valid = reinterpret_cast<uint8_t*>(vals + a.max_n);
+        tile = reinterpret_cast<float*>(sm + L.off_tile);
+        vals = reinterpret_cast<float*>(sm + L.off_vals);
+        valid = sm + L.off_valid;
+        refok = sm + L.off_refok;
         simplex_runs = 0;
+        tile_ok = false;
+        tile_on = a.tile_w > 0 && a.tile_h > 0;
+        tx0 = ty0 = 0;
+    }
+
+    // Make the tile cover every sample support of the warped subset, staging
+    // a new box with TMA when the warp has left the current one. False when
+    // the subset does not fit a box (the samples then read global memory).
+    __device__ void ensure_tile(const float W[6]) {
+        if (!tile_on) return;
+        const float h = (float)half;
+        float fx[4], fy[4];
+        const float ox[4] = {-h, h, -h, h}, oy[4] = {-h, -h, h, h};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            fx[k] = __fmaf_rn(W[0], ox[k], __fmaf_rn(W[1], oy[k], W[2]));
+            fy[k] = __fmaf_rn(W[3], ox[k], __fmaf_rn(W[4], oy[k], W[5]));
+        }
+        const float mnx = fminf(fminf(fx[0], fx[1]), fminf(fx[2], fx[3]));
+        const float mxx = fmaxf(fmaxf(fx[0], fx[1]), fmaxf(fx[2], fx[3]));
+        const float mny = fminf(fminf(fy[0], fy[1]), fminf(fy[2], fy[3]));
+        const float mxy = fmaxf(fmaxf(fy[0], fy[1]), fmaxf(fy[2], fy[3]));
+        if (!(mnx > -1e6f && mxx < 1e6f && mny > -1e6f && mxy < 1e6f)) {
+            tile_ok = false;
+            return;
+        }
+        // support of every sample, one pixel of slack for rounding
+        const int lo_tap = SIX ? 3 : 2, hi_tap = SIX ? 4 : 3;
+        const int x_lo = cx + (int)floorf(mnx) - lo_tap, x_hi = cx + (int)floorf(mxx) + hi_tap;
+        const int y_lo = cy + (int)floorf(mny) - lo_tap, y_hi = cy + (int)floorf(mxy) + hi_tap;
+        if (tile_ok && x_lo >= tx0 && x_hi < tx0 + a.tile_w && y_lo >= ty0 && y_hi < ty0 + a.tile_h) return;
+        const int need_w = x_hi - x_lo + 1, need_h = y_hi - y_lo + 1;
+        if (need_w + 3 > a.tile_w || need_h > a.tile_h) {
+            tile_ok = false;
+            return;
+        }
+        // centre the support, x start on a 16-byte boundary (a multiple of 4)
+        int nx = x_lo - (a.tile_w - 3 - need_w) / 2;
+        nx = nx >= 0 ? (nx & ~3) : -((-nx + 3) & ~3);
+        const int ny = y_lo - (a.tile_h - need_h) / 2;
+        __syncwarp();
+        if (lane == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(bar, (uint32_t)(a.tile_w * a.tile_h * 4));
+            tma_load_2d(tile, tmap, nx, ny, bar);
+        }
+        const bool done = mbar_wait_bounded(bar, phase, 1 << 22);
+        phase ^= 1u;
+        if (!__all_sync(kFull, done)) {
+            // A copy that never completed: stop staging for this warp.
+            if (lane == 0 && a.err) atomicExch(a.err, 1);
+            tile_on = false;
+            tile_ok = false;
+            return;
+        }
+        tx0 = nx;
+        ty0 = ny;
+        tile_ok = true;
     }
 
     // Walk this lane's pixels i = lane, lane + 32, ...: (row, col) in the subset.
@@ -73,6 +154,7 @@ struct WarpSolver {
     __device__ __forceinline__ void for_pixels(F&& f) const {
         int row = lane / dim, col = lane - row * dim;
         const int q = 32 / dim, r = 32 - q * dim;
+#pragma unroll 4
         for (int i = lane; i < n; i += 32) {
             f(i, row, col);
             col += r;
@@ -85,16 +167,19 @@ struct WarpSolver {
     }
 
     __device__ __forceinline__ size_t ref_idx(int row, int col) const {
-        return ref_base + (size_t)row * a.W + col;
+        return ref_base + (size_t)row * a.pitch + col;
     }
 
     // sample_warped_subset (optimization_engine.cpp:191-269) on centre +
     // offset coordinates; returns the count of valid samples, their sum in `sum`.
     __device__ int sample(const float W[6], float& sum) {
+        ensure_tile(W);
         float part = 0.0f;
         int cnt = 0;
         const float lo_x = (float)(4 - cx), hi_x = (float)(a.W - 4 - cx);
         const float lo_y = (float)(4 - cy), hi_y = (float)(a.H - 4 - cy);
+        const int lo_tap = SIX ? 2 : 1, hi_tap = SIX ? 3 : 2;
+        const bool use_tile = tile_ok;
         for_pixels([&](int i, int row, int col) {
             const float ox = (float)(col - half), oy = (float)(row - half);
             const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
@@ -105,9 +190,15 @@ struct WarpSolver {
             if (rx >= lo_x && rx < hi_x && ry >= lo_y && ry < hi_y) {
                 const float flx = floorf(fx), fly = floorf(fy);
                 const int xi = cx + (int)flx, yi = cy + (int)fly;
-                val = SIX ? interp6(a.defI, a.W, xi, yi, fx - flx, fy - fly)
-                          : interp4(a.defI, a.W, xi, yi, fx - flx, fy - fly);
-                if (!(__ldg(a.refI + ref_idx(row, col)) < kGhost)) {
+                const int lx = xi - tx0, ly = yi - ty0;
+                if (use_tile && lx >= lo_tap && lx + hi_tap < a.tile_w && ly >= lo_tap && ly + hi_tap < a.tile_h) {
+                    val = SIX ? interp6s(tile, a.tile_w, lx, ly, fx - flx, fy - fly)
+                              : interp4s(tile, a.tile_w, lx, ly, fx - flx, fy - fly);
+                } else {
+                    val = SIX ? interp6(a.defI, a.pitch, xi, yi, fx - flx, fy - fly)
+                              : interp4(a.defI, a.pitch, xi, yi, fx - flx, fy - fly);
+                }
+                if (refok[i]) {
                     ok = 1;
                     part = part + val;
                     ++cnt;
@@ -425,7 +516,7 @@ struct WarpSolver {
                 const int x = cx + (col - half) + u, y = cy + (row - half) + v;
                 if (x < 4 || x > a.W - 5 || y < 4 || y > a.H - 5) return false;
                 r = rv;
-                d = __ldg(a.defI + (size_t)y * a.W + x);
+                d = __ldg(a.defI + (size_t)y * a.pitch + x);
                 return true;
             };
             for (int i = 0; i < n; i += 9) {
@@ -506,10 +597,16 @@ struct WarpSolver {
 };
 
 template <bool SIX>
-__global__ void __launch_bounds__(kSolveThreads, 4) solve_kernel(SolveArgs a) {
-    extern __shared__ __align__(16) unsigned char smem[];
+__global__ void __launch_bounds__(kSolveThreads, 4)
+    solve_kernel(const __grid_constant__ CUtensorMap tmap, SolveArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* my = smem + (size_t)warp * a.smem_per_warp;
+    if (lane == 0) mbar_init(reinterpret_cast<uint64_t*>(my), 1);
+    fence_proxy_async_smem();
+    __syncwarp();
+    uint32_t phase = 0;
+    bool tile_on = a.tile_w > 0;
     const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
     for (;;) {
         int t = 0;
@@ -530,7 +627,8 @@ __global__ void __launch_bounds__(kSolveThreads, 4) solve_kernel(SolveArgs a) {
             if (lane == 0) a.results[t] = out;
             continue;
         }
-        WarpSolver<SIX> s(a, lane, my);
+        WarpSolver<SIX> s(a, lane, my, &tmap, phase);
+        s.tile_on = tile_on;
         s.cx = T.cx;
         s.cy = T.cy;
         s.dim = dim;
@@ -540,17 +638,21 @@ __global__ void __launch_bounds__(kSolveThreads, 4) solve_kernel(SolveArgs a) {
         s.mref = ms.x;
         s.iref = 1.0f / ms.y;
         s.min_valid = (int)((float)s.n * kMinValidPixelFraction);
-        s.ref_base = (size_t)(T.cy - half) * a.W + (T.cx - half);
+        s.ref_base = (size_t)(T.cy - half) * a.pitch + (T.cx - half);
 
         int ghost = 0;
-        s.for_pixels([&](int, int row, int col) {
-            if (__ldg(a.refI + s.ref_idx(row, col)) < kGhost) ++ghost;
+        s.for_pixels([&](int i, int row, int col) {
+            const bool g = __ldg(a.refI + s.ref_idx(row, col)) < kGhost;
+            s.refok[i] = g ? 0 : 1;
+            if (g) ++ghost;
         });
         ghost = wsum(ghost);
         s.step_matrix(a.pool_Hs + (size_t)T.node * 21);
 
         int trigger = 0;
         Res r = s.solve(T.g, T.mode, trigger);
+        phase = s.phase;
+        tile_on = s.tile_on;
         if ((float)ghost / (float)(dim * dim) > kGhostRejectFraction) {
             r.score = 2.0f;
             r.status = 1;
@@ -571,24 +673,67 @@ __global__ void __launch_bounds__(kSolveThreads, 4) solve_kernel(SolveArgs a) {
 
 }  // namespace
 
-size_t solve_smem_per_warp(int max_n) {
-    size_t b = 2 * 36 * sizeof(double) + (size_t)max_n * sizeof(float) + (size_t)max_n;
-    return (b + 15) & ~(size_t)15;
+void tile_box(int dim, int six, int& tw, int& th) {
+    // the subset's support plus one pixel of rounding slack each side, three
+    // columns of alignment slack, and a margin of two pixels for the warp to
+    // move in before the tile is staged again
+    const int need = dim + (six ? 5 : 3) + 2;
+    tw = ((need + 3 + 4) + 3) & ~3;
+    th = need + 4;
+    if (tw > 256 || th > 256) tw = th = 0;
 }
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+}  // namespace
 
 cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStream_t st) {
     SolveArgs a = a0;
-    a.smem_per_warp = solve_smem_per_warp(a.max_n);
+    CUtensorMap tmap;
+    std::memset(&tmap, 0, sizeof(tmap));
+    int tw = 0, th = 0;
+    tile_box(a.dim, six, tw, th);
+    const bool pitch_ok = (a.pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(a.defI) % 16) == 0;
+    PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+    if (tw > 0 && pitch_ok && enc) {
+        const cuuint64_t gdim[2] = {(cuuint64_t)a.W, (cuuint64_t)a.H};
+        const cuuint64_t gstride[1] = {(cuuint64_t)a.pitch * 4};
+        const cuuint32_t box[2] = {(cuuint32_t)tw, (cuuint32_t)th};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = enc(&tmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.defI), gdim, gstride,
+                               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) tw = th = 0;
+    } else {
+        tw = th = 0;
+    }
+    a.tile_w = tw;
+    a.tile_h = th;
+    a.smem_per_warp = smem_layout(a.max_n, tw, th).bytes;
     const size_t smem = a.smem_per_warp * (kSolveThreads / 32);
     cudaError_t e;
     if (six) {
         e = cudaFuncSetAttribute(solve_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        solve_kernel<true><<<grid_blocks, kSolveThreads, smem, st>>>(a);
+        solve_kernel<true><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
     } else {
         e = cudaFuncSetAttribute(solve_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        solve_kernel<false><<<grid_blocks, kSolveThreads, smem, st>>>(a);
+        solve_kernel<false><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
     }
     return cudaGetLastError();
 }

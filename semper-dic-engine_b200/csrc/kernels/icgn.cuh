@@ -16,6 +16,7 @@ struct SolveArgs {
     const float* refGy;
     const float* defI;   // deformed intensities
     int W, H;
+    int pitch;           // row pitch of every plane, elements (a multiple of 4 for TMA)
     const uint8_t* pool_valid;  // Hessian pool, indexed by dic_task.node
     const float2* pool_ms;      // (mean, std)
     const double* pool_Hs;      // whole-subset step matrix, 21 doubles per node (upper triangle)
@@ -28,10 +29,25 @@ struct SolveArgs {
     dic_result* results;     // one per task
     int* queue;              // work counter, zero before the launch
     const int* cancel;       // host-mapped cancel flag polled per task, or null
+    int* err;                // set to 1 when a TMA wait ran out (the warp then reads global memory)
     size_t smem_per_warp;    // set by launch_solve
+    int tile_w, tile_h;      // TMA box of the deformed tile, set by launch_solve (0: no tile)
 };
 
-size_t solve_smem_per_warp(int max_n);
+struct SmemLayout {
+    size_t off_h, off_tile, off_vals, off_valid, off_refok, bytes;
+};
+__host__ __device__ inline SmemLayout smem_layout(int max_n, int tile_w, int tile_h) {
+    SmemLayout L;
+    L.off_h = 16;
+    L.off_tile = 640;  // 16 + 2 * 36 * 8 = 592, rounded up to 128
+    L.off_vals = L.off_tile + (((size_t)tile_w * tile_h * 4 + 127) & ~(size_t)127);
+    L.off_valid = L.off_vals + (size_t)max_n * 4;
+    L.off_refok = L.off_valid + (size_t)max_n;
+    L.bytes = (L.off_refok + (size_t)max_n + 127) & ~(size_t)127;
+    return L;
+}
+void tile_box(int dim, int six, int& tw, int& th);
 cudaError_t launch_solve(const SolveArgs& a, int six, int grid_blocks, cudaStream_t st);
 
 }  // namespace dic

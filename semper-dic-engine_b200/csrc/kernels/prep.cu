@@ -21,11 +21,13 @@ namespace {
 // the gradient the correctly rounded quotient in any order. Stores are float4
 // when the row pitch allows it (W % 4 == 0), scalar otherwise.
 __global__ void image_kernel(const uint8_t* __restrict__ px, const uint8_t* __restrict__ mask, int W,
-                             int H, float* __restrict__ I, float* __restrict__ gx, float* __restrict__ gy) {
+                             int H, int pitch, float* __restrict__ I, float* __restrict__ gx,
+                             float* __restrict__ gy) {
     const int x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
     const int y = blockIdx.y;
-    if (x0 >= W || y >= H) return;
+    if (x0 >= pitch || y >= H) return;
     const size_t row = (size_t)y * W;
+    const size_t orow = (size_t)y * pitch;
     float vi[4], vx[4], vy[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -44,17 +46,17 @@ __global__ void image_kernel(const uint8_t* __restrict__ px, const uint8_t* __re
         }
         if (mask && __ldg(mask + p) < 128) vi[k] = -10.0f;
     }
-    if ((W & 3) == 0) {
-        reinterpret_cast<float4*>(I + row)[x0 >> 2] = make_float4(vi[0], vi[1], vi[2], vi[3]);
-        reinterpret_cast<float4*>(gx + row)[x0 >> 2] = make_float4(vx[0], vx[1], vx[2], vx[3]);
-        reinterpret_cast<float4*>(gy + row)[x0 >> 2] = make_float4(vy[0], vy[1], vy[2], vy[3]);
+    if ((pitch & 3) == 0) {
+        reinterpret_cast<float4*>(I + orow)[x0 >> 2] = make_float4(vi[0], vi[1], vi[2], vi[3]);
+        reinterpret_cast<float4*>(gx + orow)[x0 >> 2] = make_float4(vx[0], vx[1], vx[2], vx[3]);
+        reinterpret_cast<float4*>(gy + orow)[x0 >> 2] = make_float4(vy[0], vy[1], vy[2], vy[3]);
     } else {
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            if (x0 + k >= W) break;
-            I[row + x0 + k] = vi[k];
-            gx[row + x0 + k] = vx[k];
-            gy[row + x0 + k] = vy[k];
+            if (x0 + k >= pitch) break;
+            I[orow + x0 + k] = vi[k];
+            gx[orow + x0 + k] = vx[k];
+            gy[orow + x0 + k] = vy[k];
         }
     }
 }
@@ -88,7 +90,7 @@ __global__ void scan_kernel(const uint8_t* __restrict__ mask, int W, int H, int 
 // lane partial sums + butterfly), the 21-entry Gauss-Newton Hessian (FP64),
 // then the 2x2 and scaled-rcond checks on lane 0.
 __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict__ Gx,
-                            const float* __restrict__ Gy, int W, int H, const uint8_t* __restrict__ skip,
+                            const float* __restrict__ Gy, int W, int H, int pitch, const uint8_t* __restrict__ skip,
                             int gridW, int gridH, int rect_x, int rect_y, int step, int dim, int lm,
                             uint8_t* __restrict__ valid, float2* __restrict__ ms, double* __restrict__ H21,
                             double* __restrict__ Hs21) {
@@ -110,7 +112,7 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
         }
         return;
     }
-    const size_t base = (size_t)(cy - half) * W + (cx - half);
+    const size_t base = (size_t)(cy - half) * pitch + (cx - half);
     const int q = 32 / dim, r = 32 - q * dim;
 
     float part = 0.0f;
@@ -118,7 +120,7 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     {
         int row = lane / dim, col = lane - row * dim;
         for (int i = lane; i < n; i += 32) {
-            const float v = __ldg(I + base + (size_t)row * W + col);
+            const float v = __ldg(I + base + (size_t)row * pitch + col);
             if (!(v < -5.0f)) {
                 part = part + v;
                 ++cnt;
@@ -145,7 +147,7 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     {
         int row = lane / dim, col = lane - row * dim;
         for (int i = lane; i < n; i += 32) {
-            const float v = __ldg(I + base + (size_t)row * W + col);
+            const float v = __ldg(I + base + (size_t)row * pitch + col);
             if (!(v < -5.0f)) {
                 const float d = v - mean;
                 part = __fmaf_rn(d, d, part);
@@ -164,7 +166,7 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     {
         int row = lane / dim, col = lane - row * dim;
         for (int i = lane; i < n; i += 32) {
-            const size_t p = base + (size_t)row * W + col;
+            const size_t p = base + (size_t)row * pitch + col;
             if (!(__ldg(I + p) < -5.0f)) {
                 const float g0 = __ldg(Gx + p) * inv, g1 = __ldg(Gy + p) * inv;
                 const float fx = (float)(col - half), fy = (float)(row - half);
@@ -220,12 +222,12 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
 
 }  // namespace
 
-cudaError_t launch_image_prep(const uint8_t* px, const uint8_t* mask, int W, int H, float* I, float* gx,
+cudaError_t launch_image_prep(const uint8_t* px, const uint8_t* mask, int W, int H, int pitch, float* I, float* gx,
                               float* gy, cudaStream_t st) {
     const int threads = 128;
-    const int per_row = (W + 3) / 4;
+    const int per_row = (pitch + 3) / 4;
     dim3 grid((per_row + threads - 1) / threads, H);
-    image_kernel<<<grid, threads, 0, st>>>(px, mask, W, H, I, gx, gy);
+    image_kernel<<<grid, threads, 0, st>>>(px, mask, W, H, pitch, I, gx, gy);
     return cudaGetLastError();
 }
 
@@ -238,12 +240,12 @@ cudaError_t launch_grid_scan(const uint8_t* mask, int W, int H, int gridW, int g
     return cudaGetLastError();
 }
 
-cudaError_t launch_pool(const float* I, const float* gx, const float* gy, int W, int H, const uint8_t* skip,
+cudaError_t launch_pool(const float* I, const float* gx, const float* gy, int W, int H, int pitch, const uint8_t* skip,
                         int gridW, int gridH, int rect_x, int rect_y, int step, int dim, int lm, uint8_t* valid,
                         float2* ms, double* H21, double* Hs21, cudaStream_t st) {
     const int nodes = gridW * gridH;
     const int wpb = 4;
-    pool_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(I, gx, gy, W, H, skip, gridW, gridH, rect_x,
+    pool_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(I, gx, gy, W, H, pitch, skip, gridW, gridH, rect_x,
                                                                rect_y, step, dim, lm, valid, ms, H21, Hs21);
     return cudaGetLastError();
 }

@@ -93,10 +93,10 @@ def lib():
         L.semper_b200_stream.restype = _vp
         L.semper_b200_last_timings.argtypes = [_vp, _f32p, ctypes.POINTER(ctypes.c_longlong)]
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
-        L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 2 + [_vp] * 4
+        L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 3 + [_vp] * 4
         L.dic_cuda_grid_scan.argtypes = [_vp] + [ctypes.c_int] * 8 + [_vp, _vp, _vp]
-        L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 2 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
-        L.dic_cuda_solve.argtypes = [_vp] * 4 + [ctypes.c_int] * 2 + [_vp] * 3 + [ctypes.c_int] * 3 + \
+        L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 3 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
+        L.dic_cuda_solve.argtypes = [_vp] * 4 + [ctypes.c_int] * 3 + [_vp] * 3 + [ctypes.c_int] * 3 + \
             [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]
         L.dic_cuda_median_pass.argtypes = [ctypes.c_int] * 2 + [_vp] * 6
         L.dic_cuda_clear_failed.argtypes = [ctypes.c_int, _vp, _vp, _vp]
@@ -312,14 +312,23 @@ def _ck(rc, what):
         raise RuntimeError(f"{what} failed with CUDA error {rc}")
 
 
+def pitch_of(width: int) -> int:
+    """Row pitch (elements) of the float planes: rows padded to 16 bytes."""
+    return (width + 3) & ~3
+
+
 def image_prep(px, mask=None):
+    """Float planes (I, gx, gy) of an 8-bit image, rows pitched to 16 bytes:
+    tensors of shape (h, pitch); columns >= w are zero."""
     import torch
 
     h, w = px.shape
-    I = torch.empty((h, w), dtype=torch.float32, device=px.device)
+    P = pitch_of(w)
+    I = torch.empty((h, P), dtype=torch.float32, device=px.device)
     gx = torch.empty_like(I)
     gy = torch.empty_like(I)
-    _ck(lib().dic_cuda_image_prep(_ptr(px), _ptr(mask), w, h, _ptr(I), _ptr(gx), _ptr(gy), _stream()), "image_prep")
+    _ck(lib().dic_cuda_image_prep(_ptr(px), _ptr(mask), w, h, P, _ptr(I), _ptr(gx), _ptr(gy), _stream()),
+        "image_prep")
     return I, gx, gy
 
 
@@ -334,36 +343,37 @@ def grid_scan(mask, w, h, grid, rect, step, subset):
     return skip, nv
 
 
-def hessian_pool(I, gx, gy, skip, grid, rect, step, subset, lm=True):
+def hessian_pool(planes, width, skip, grid, rect, step, subset, lm=True):
     import torch
 
-    h, w = I.shape
+    I, gx, gy = planes
+    h, P = I.shape
     gw, gh = grid
     n = gw * gh
     valid = torch.empty(n, dtype=torch.uint8, device="cuda")
     ms = torch.empty((n, 2), dtype=torch.float32, device="cuda")
     H = torch.empty((n, 21), dtype=torch.float64, device="cuda")
     Hs = torch.empty((n, 21), dtype=torch.float64, device="cuda")
-    _ck(lib().dic_cuda_hessian_pool(_ptr(I), _ptr(gx), _ptr(gy), w, h, _ptr(skip), gw, gh, rect[0], rect[1], step,
-                                    subset, 1 if lm else 0, _ptr(valid), _ptr(ms), _ptr(H), _ptr(Hs), _stream()),
-        "hessian_pool")
+    _ck(lib().dic_cuda_hessian_pool(_ptr(I), _ptr(gx), _ptr(gy), width, h, P, _ptr(skip), gw, gh, rect[0], rect[1],
+                                    step, subset, 1 if lm else 0, _ptr(valid), _ptr(ms), _ptr(H), _ptr(Hs),
+                                    _stream()), "hessian_pool")
     return valid, ms, H, Hs
 
 
-def solve(ref_planes, def_I, pool, subset, tasks: np.ndarray, lm=True, six=False, blocks=0):
+def solve(ref_planes, def_I, width, pool, subset, tasks: np.ndarray, lm=True, six=False, blocks=0):
     """tasks: TASK_DT array (node indexes into pool). Returns RESULT_DT array."""
     import torch
 
     rI, rgx, rgy = ref_planes
     valid, ms, _H, Hs = pool
-    h, w = rI.shape
+    h, P = rI.shape
     n = len(tasks)
     tbytes = torch.from_numpy(np.ascontiguousarray(tasks).view(np.uint8).copy()).cuda()
     res = torch.zeros(n * RESULT_DT.itemsize, dtype=torch.uint8, device="cuda")
     q = torch.zeros(1, dtype=torch.int32, device="cuda")
-    _ck(lib().dic_cuda_solve(_ptr(rI), _ptr(rgx), _ptr(rgy), _ptr(def_I), w, h, _ptr(valid), _ptr(ms), _ptr(Hs),
-                             subset, 1 if lm else 0, 1 if six else 0, _ptr(tbytes), n, _ptr(res), _ptr(q), blocks,
-                             _stream()), "solve")
+    _ck(lib().dic_cuda_solve(_ptr(rI), _ptr(rgx), _ptr(rgy), _ptr(def_I), width, h, P, _ptr(valid), _ptr(ms),
+                             _ptr(Hs), subset, 1 if lm else 0, 1 if six else 0, _ptr(tbytes), n, _ptr(res), _ptr(q),
+                             blocks, _stream()), "solve")
     torch.cuda.synchronize()
     return res.cpu().numpy().view(RESULT_DT).copy()
 
