@@ -213,3 +213,13 @@ def test_return_codes():
     assert e.run(dfm, sb.params((0, 0, 256, 256), 8, 15, 8))[0] == sb.SEMPER_ERR_STRAIN_WINDOW
     assert e.run(dfm, sb.params((300, 0, 10, 10), 8, 15, 15))[0] == sb.SEMPER_ERR_ROI
     assert e.run(dfm[:100], prm)[0] == sb.SEMPER_ERR_INIT
+
+
+def test_pipeline_unpadded_width_bit_exact():
+    # width not a multiple of 4: the device planes carry a padded pitch
+    w, h = 330, 300
+    ref = sb.speckle(w, h, 21)
+    dfm = sb.speckle(w, h, 21, sb.warp_block(cx=165, cy=150, u0=-1.2, v0=0.6, a=(0.004, 0.0, 0.0, 0.003)), 1.0, 3)
+    d, o = _run_both(ref, dfm, sb.params((0, 0, w, h), 9, 21, 27))
+    assert o[0] > 100
+    _assert_field_equal(d, o)
