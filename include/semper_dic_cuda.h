@@ -54,12 +54,18 @@ int dic_cuda_hessian_pool(const float* d_I, const float* d_gx, const float* d_gy
    (src/math/optimization_engine.cpp:55-118) with IC-GN (:272-465), the
    Simplex rescue (:531-651) and the coarse search (:120-179) as the task's
    mode asks, then the Ghost Wall rejection. Pool arrays are indexed by
-   dic_task.node. d_queue is a work counter that must be zero at launch.
+   dic_task.node. Two passes run on the stream: the common case (whole-subset
+   iterations, no Simplex) for every task, then every path for the tasks the
+   first pass handed on. d_scratch holds their work counters and list
+   (dic_cuda_solve_scratch_bytes); its contents need no initialisation.
    `blocks` = persistent grid size (0 = one wave). */
 int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const float* d_ref_gy, const float* d_def_I,
                    int width, int height, int pitch, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
                    const double* d_pool_Hs21, int subset, int lm, int six, const dic_task* d_tasks, int n_tasks,
-                   dic_result* d_results, int* d_queue, int blocks, void* stream);
+                   dic_result* d_results, void* d_scratch, int blocks, void* stream);
+
+/* Bytes of scratch dic_cuda_solve needs for n_tasks tasks. */
+size_t dic_cuda_solve_scratch_bytes(int n_tasks);
 
 /* One pass of StrainCalculator::reject_displacement_outliers
    (src/strain/strain_calculator.cpp:174-224): d_fail from the flags d_ok of

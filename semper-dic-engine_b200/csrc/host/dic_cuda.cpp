@@ -36,7 +36,7 @@ DIC_API int dic_cuda_hessian_pool(const float* d_I, const float* d_gx, const flo
 DIC_API int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const float* d_ref_gy, const float* d_def_I,
                            int width, int height, int pitch, const uint8_t* d_pool_valid, const float* d_pool_mean_std,
                            const double* d_pool_Hs21, int subset, int lm, int six, const dic_task* d_tasks,
-                           int n_tasks, dic_result* d_results, int* d_queue, int blocks, void* stream) {
+                           int n_tasks, dic_result* d_results, void* d_scratch, int blocks, void* stream) {
     if (n_tasks <= 0) return 0;
     dic::SolveArgs a{};
     a.refI = d_ref_I;
@@ -56,7 +56,8 @@ DIC_API int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const fl
     a.tasks = d_tasks;
     a.n_tasks = n_tasks;
     a.results = d_results;
-    a.queue = d_queue;
+    a.queue = reinterpret_cast<int*>(d_scratch);
+    a.deferred = reinterpret_cast<int*>(d_scratch) + 4;
     if (blocks <= 0) {
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
@@ -66,6 +67,8 @@ DIC_API int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const fl
     }
     return (int)dic::launch_solve(a, six, blocks, S(stream));
 }
+
+DIC_API size_t dic_cuda_solve_scratch_bytes(int n_tasks) { return (size_t)(4 + (n_tasks > 0 ? n_tasks : 0)) * 4; }
 
 DIC_API int dic_cuda_median_pass(int grid_w, int grid_h, const float* d_u, const float* d_v, const uint8_t* d_ok,
                                  uint8_t* d_fail, int* d_n_fail, void* stream) {

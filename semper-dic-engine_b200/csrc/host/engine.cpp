@@ -229,7 +229,9 @@ struct Engine::Impl {
     DevBuf<uint8_t> in_mesh;
     DevBuf<dic_task> tasks;
     DevBuf<dic_result> results;
-    DevBuf<int> counters;  // [0] queue [1] n_tasks [2] n_valid [3] n_fail [4] n_drop [5..6] emit [7] n_boundary
+    DevBuf<int> counters;  // [1] n_tasks [2] n_valid [3] n_fail [4] n_drop [5..6] emit [7] n_boundary [9] TMA error
+    DevBuf<int> solve_q;   // the solve's work counters
+    DevBuf<int> deferred;  // tasks the fast solve pass leaves to the general one
     DevBuf<dic::PathStats> pstats;
     DevBuf<dic::BoundarySeed> bseeds;
     DevBuf<dic::ScatterRec> scat;
@@ -273,6 +275,7 @@ struct Engine::Impl {
         a.max_n = dim * dim;
         a.lm = 1;
         a.cancel = E.d_cancel_;
+        a.queue = solve_q.p;
         (void)six;
         return a;
     }
@@ -290,16 +293,16 @@ struct Engine::Impl {
         if (tk.empty()) return out;
         tasks.ensure(std::max(tasks.n, tk.size()));
         results.ensure(std::max(results.n, tk.size()));
+        deferred.ensure(std::max(deferred.n, tk.size()));
         check(cudaMemcpyAsync(tasks.p, tk.data(), tk.size() * sizeof(dic_task), cudaMemcpyHostToDevice, E.stream_),
               "H2D tasks");
-        check(cudaMemsetAsync(counters.p, 0, sizeof(int), E.stream_), "queue reset");
         dic::SolveArgs a = solve_args(p.subset_size, p.six);
         a.tasks = tasks.p;
         a.n_tasks = (int)tk.size();
         a.n_tasks_dev = nullptr;
         a.results = results.p;
-        a.queue = counters.p;
-        launched(1, dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)tk.size()), E.stream_), "solve");
+        a.deferred = deferred.p;
+        launched(2, dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)tk.size()), E.stream_), "solve");
         check(cudaMemcpyAsync(out.data(), results.p, tk.size() * sizeof(dic_result), cudaMemcpyDeviceToHost,
                               E.stream_),
               "D2H results");
@@ -335,6 +338,7 @@ Engine::Engine() : impl_(new Impl(*this)) {
     check(cudaDeviceGetAttribute(&impl_->sm_count, cudaDevAttrMultiProcessorCount, dev), "SM count");
     for (auto& e : impl_->ev) check(cudaEventCreate(&e), "event");
     impl_->counters.ensure(16);
+    impl_->solve_q.ensure(4);
     impl_->pstats.ensure(1);
 }
 
@@ -850,6 +854,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         const auto t_a = clk::now();
         tasks.ensure(std::max(tasks.n, NG));
         results.ensure(std::max(results.n, NG));
+        deferred.ensure(std::max(deferred.n, NG));
         check(cudaMemsetAsync(counters.p, 0, 2 * sizeof(int), st), "counters");
         check(cudaMemsetAsync(pstats.p, 0, sizeof(dic::PathStats), st), "stats");
         launched(1, dic::launch_path_a_tasks(gW, gH, params.rect_x, params.rect_y, params.step, fsolved.p, ftag.p, mesh(),
@@ -864,9 +869,9 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             a.n_tasks_dev = counters.p + 1;
             a.n_tasks = n_a;
             a.results = results.p;
-            a.queue = counters.p;
+            a.deferred = deferred.p;
             check(cudaEventRecord(ev[5], st), "event");
-            launched(1, dic::launch_solve(a, params.six ? 1 : 0, solve_grid(n_a), st), "path A solve");
+            launched(2, dic::launch_solve(a, params.six ? 1 : 0, solve_grid(n_a), st), "path A solve");
             check(cudaEventRecord(ev[6], st), "event");
             launched(1, dic::launch_commit(tasks.p, counters.p + 1, n_a, results.p, field(), pstats.p, st), "path A commit");
         }

@@ -27,11 +27,15 @@ struct SolveArgs {
     const int* n_tasks_dev;  // task count in device memory, or null to use n_tasks
     int n_tasks;
     dic_result* results;     // one per task
-    int* queue;              // work counter, zero before the launch
+    int* queue;              // 3 work counters (zeroed by launch_solve)
+    int* deferred;           // n_tasks slots: tasks the fast pass leaves to the general one
     const int* cancel;       // host-mapped cancel flag polled per task, or null
     int* err;                // set to 1 when a TMA wait ran out (the warp then reads global memory)
     size_t smem_per_warp;    // set by launch_solve
     int tile_w, tile_h;      // TMA box of the deformed tile, set by launch_solve (0: no tile)
+    // set by launch_solve from dim and the shared-memory layout
+    int half, n, min_valid;
+    int off_tile, off_vals, off_valid, off_refok;
 };
 
 struct SmemLayout {
@@ -39,8 +43,8 @@ struct SmemLayout {
 };
 __host__ __device__ inline SmemLayout smem_layout(int max_n, int tile_w, int tile_h) {
     SmemLayout L;
-    L.off_h = 16;
-    L.off_tile = 640;  // 16 + 2 * 36 * 8 = 592, rounded up to 128
+    L.off_h = 64;      // barrier (8 B) at 0, tile state at 16
+    L.off_tile = 640;  // 64 + 2 * 36 * 8 = 640
     L.off_vals = L.off_tile + (((size_t)tile_w * tile_h * 4 + 127) & ~(size_t)127);
     L.off_valid = L.off_vals + (size_t)max_n * 4;
     L.off_refok = L.off_valid + (size_t)max_n;
@@ -48,6 +52,8 @@ __host__ __device__ inline SmemLayout smem_layout(int max_n, int tile_w, int til
     return L;
 }
 void tile_box(int dim, int six, int& tw, int& th);
+// Two launches on `st`: the fast pass over every task, then the general pass
+// over the tasks it deferred. Scratch: queue (3 ints) and deferred (n ints).
 cudaError_t launch_solve(const SolveArgs& a, int six, int grid_blocks, cudaStream_t st);
 
 }  // namespace dic

@@ -38,6 +38,7 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
                "semper_b200_stream"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
+               "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
                "dic_cuda_pack"]
 
@@ -98,6 +99,8 @@ def lib():
         L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 3 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
         L.dic_cuda_solve.argtypes = [_vp] * 4 + [ctypes.c_int] * 3 + [_vp] * 3 + [ctypes.c_int] * 3 + \
             [_vp, ctypes.c_int, _vp, _vp, ctypes.c_int, _vp]
+        L.dic_cuda_solve_scratch_bytes.argtypes = [ctypes.c_int]
+        L.dic_cuda_solve_scratch_bytes.restype = ctypes.c_size_t
         L.dic_cuda_median_pass.argtypes = [ctypes.c_int] * 2 + [_vp] * 6
         L.dic_cuda_clear_failed.argtypes = [ctypes.c_int, _vp, _vp, _vp]
         L.dic_cuda_vsg.argtypes = [ctypes.c_int] * 4 + [_vp] * 7
@@ -370,10 +373,10 @@ def solve(ref_planes, def_I, width, pool, subset, tasks: np.ndarray, lm=True, si
     n = len(tasks)
     tbytes = torch.from_numpy(np.ascontiguousarray(tasks).view(np.uint8).copy()).cuda()
     res = torch.zeros(n * RESULT_DT.itemsize, dtype=torch.uint8, device="cuda")
-    q = torch.zeros(1, dtype=torch.int32, device="cuda")
+    scratch = torch.empty(lib().dic_cuda_solve_scratch_bytes(n), dtype=torch.uint8, device="cuda")
     _ck(lib().dic_cuda_solve(_ptr(rI), _ptr(rgx), _ptr(rgy), _ptr(def_I), width, h, P, _ptr(valid), _ptr(ms),
-                             _ptr(Hs), subset, 1 if lm else 0, 1 if six else 0, _ptr(tbytes), n, _ptr(res), _ptr(q),
-                             blocks, _stream()), "solve")
+                             _ptr(Hs), subset, 1 if lm else 0, 1 if six else 0, _ptr(tbytes), n, _ptr(res),
+                             _ptr(scratch), blocks, _stream()), "solve")
     torch.cuda.synchronize()
     return res.cpu().numpy().view(RESULT_DT).copy()
 
