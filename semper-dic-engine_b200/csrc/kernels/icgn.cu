@@ -43,6 +43,8 @@ namespace dic {
 namespace {
 
 constexpr int kPixelUnroll = DIC_PIXEL_UNROLL;
+constexpr int kArgsBytes = 256;  // shared-memory header: the block's copy of SolveArgs
+static_assert(sizeof(SolveArgs) <= kArgsBytes, "SolveArgs header");
 constexpr float kCorrSimplexTrigger = 0.4f;
 constexpr float kSimplexFailScore = 0.1f;
 constexpr float kLmAlpha = 0.05f;
@@ -64,8 +66,10 @@ struct TileState {
 };
 
 // The per-subset values of a solve. Launch constants (plane pointers, image
-// and subset sizes, offsets into shared memory) are read from the kernel's
-// __grid_constant__ arguments where they are used, so they take no registers.
+// and subset sizes, offsets into shared memory) are read where they are used
+// from the block's copy of the launch arguments in shared memory, so they take
+// no registers. The argument block itself is a plain by-value parameter whose
+// address is never taken.
 struct Ctx {
     const SolveArgs* a;
     unsigned char* sm;  // the warp's shared memory
@@ -127,18 +131,20 @@ __device__ __forceinline__ void ensure_tile(const Ctx& c, const float W[6]) {
     TileState* ts = state_of(c);
     if (!ts->on) return;
     const float h = (float)c.a->half;
-    float mnx = 3.0e38f, mxx = -3.0e38f, mny = 3.0e38f, mxy = -3.0e38f;
+    float mnx = 0.0f, mxx = 0.0f, mny = 0.0f, mxy = 0.0f;
+    bool in_range = true;  // every corner finite and within 1e6 px (a NaN fails the comparisons)
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const float ox = (k & 1) ? h : -h, oy = (k & 2) ? h : -h;
         const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
         const float fy = __fmaf_rn(W[3], ox, __fmaf_rn(W[4], oy, W[5]));
-        mnx = fminf(mnx, fx);
-        mxx = fmaxf(mxx, fx);
-        mny = fminf(mny, fy);
-        mxy = fmaxf(mxy, fy);
+        in_range = in_range && fx > -1e6f && fx < 1e6f && fy > -1e6f && fy < 1e6f;
+        mnx = k ? fminf(mnx, fx) : fx;
+        mxx = k ? fmaxf(mxx, fx) : fx;
+        mny = k ? fminf(mny, fy) : fy;
+        mxy = k ? fmaxf(mxy, fy) : fy;
     }
-    if (!(mnx > -1e6f && mxx < 1e6f && mny > -1e6f && mxy < 1e6f)) {
+    if (!in_range) {
         __syncwarp();
         if (c.lane == 0) ts->ok = 0;
         __syncwarp();
@@ -605,10 +611,15 @@ __device__ __noinline__ float2 coarse(Ctx c, float gu, float gv) {
 // deferred tasks, with every path.
 template <bool SIX, bool FAST>
 __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
-    solve_kernel(const __grid_constant__ CUtensorMap tmap, const __grid_constant__ SolveArgs a) {
+    solve_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char* my = smem + (size_t)warp * a.smem_per_warp;
+    // the block's copy of the launch arguments (a by-value copy: the parameter's
+    // address is never taken), read by the per-subset code through Ctx::a
+    SolveArgs* sa = reinterpret_cast<SolveArgs*>(smem);
+    if (threadIdx.x == 0) *sa = a;
+    __syncthreads();
+    unsigned char* my = smem + kArgsBytes + (size_t)warp * a.smem_per_warp;
     if (lane == 0) {
         mbar_init(reinterpret_cast<uint64_t*>(my), 1);
         TileState* ts = reinterpret_cast<TileState*>(my + 16);
@@ -621,10 +632,12 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
     __syncwarp();
     const int ntasks = FAST ? (a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks) : *(volatile const int*)(a.queue + 2);
     int* queue = FAST ? a.queue : a.queue + 1;
-    auto defer_task = [&](int t) {
+    int* const n_deferred = a.queue + 2;
+    int* const deferred = a.deferred;
+    auto defer_task = [n_deferred, deferred, lane](int t) {
         if (lane == 0) {
-            const int slot = atomicAdd(a.queue + 2, 1);
-            a.deferred[slot] = t;
+            const int slot = atomicAdd(n_deferred, 1);
+            deferred[slot] = t;
         }
         __syncwarp();
     };
@@ -655,7 +668,7 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
             continue;
         }
         Ctx c;
-        c.a = &a;
+        c.a = sa;
         c.sm = my;
         c.tmap = &tmap;
         c.cx = T.cx;
@@ -800,7 +813,7 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     a.off_vals = (int)L.off_vals;
     a.off_valid = (int)L.off_valid;
     a.off_refok = (int)L.off_refok;
-    const size_t smem = a.smem_per_warp * (kSolveThreads / 32);
+    const size_t smem = kArgsBytes + a.smem_per_warp * (kSolveThreads / 32);
     // queue[0]: fast pass, queue[1]: general pass, queue[2]: deferred count
     cudaError_t e = cudaMemsetAsync(a.queue, 0, 3 * sizeof(int), st);
     if (e != cudaSuccess) return e;
