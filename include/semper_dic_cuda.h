@@ -67,6 +67,27 @@ int dic_cuda_solve(const float* d_ref_I, const float* d_ref_gx, const float* d_r
 /* Bytes of scratch dic_cuda_solve needs for n_tasks tasks. */
 size_t dic_cuda_solve_scratch_bytes(int n_tasks);
 
+/* No counterpart in the reference: an addition of this library for callers
+   that cannot allocate device memory (a plugin living in a host
+   application's memory pool, a process under a fixed device-memory budget,
+   code that must not call cudaMalloc mid-run). Same solve, arguments and
+   results as dic_cuda_solve, without d_scratch: the scratch is a fixed array
+   in the library's device image (4 MiB per GPU that loads the library, held
+   until exit), so the call allocates nothing.
+   - n_tasks above DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS returns
+     cudaErrorInvalidValue (1) and launches nothing.
+   - The first call on a device looks up the array's device address with that
+     device current; make that first call before any stream capture.
+   - Every call shares the one array (the counters are zeroed on `stream` at
+     the start of each call): calls whose work overlaps on the GPU, on
+     different streams or from different threads, race and must be
+     serialised by the caller. */
+#define DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS 1048576
+int dic_cuda_solve_noalloc(const float* d_ref_I, const float* d_ref_gx, const float* d_ref_gy, const float* d_def_I,
+                           int width, int height, int pitch, const uint8_t* d_pool_valid,
+                           const float* d_pool_mean_std, const double* d_pool_Hs21, int subset, int lm, int six,
+                           const dic_task* d_tasks, int n_tasks, dic_result* d_results, int blocks, void* stream);
+
 /* One pass of StrainCalculator::reject_displacement_outliers
    (src/strain/strain_calculator.cpp:174-224): d_fail from the flags d_ok of
    finished passes; *d_n_fail += failures (zero it first). */
