@@ -51,6 +51,7 @@ constexpr float kLmAlpha = 0.05f;
 constexpr int kIcgnMaxIter = 50;
 constexpr float kGhostRejectFraction = 0.05f;
 constexpr float kGhost = -5.0f;
+constexpr int kCancelPollTasks = 32;  // a power of two
 
 struct Res {
     float u, v, ux, uy, vx, vy, score;
@@ -630,7 +631,8 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
     }
     fence_proxy_async_smem();
     __syncwarp();
-    const int ntasks = FAST ? (a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks) : *(volatile const int*)(a.queue + 2);
+    const int all_tasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
+    const int ntasks = (FAST || a.general_all) ? all_tasks : *(volatile const int*)(a.queue + 2);
     int* queue = FAST ? a.queue : a.queue + 1;
     int* const n_deferred = a.queue + 2;
     int* const deferred = a.deferred;
@@ -641,13 +643,16 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
         }
         __syncwarp();
     };
+    int polled = 0;
     for (;;) {
         int q = 0;
         if (lane == 0) q = atomicAdd(queue, 1);
         q = __shfl_sync(kFull, q, 0);
         if (q >= ntasks) break;
-        if (a.cancel && *(volatile const int*)a.cancel) break;
-        const int t = FAST ? q : a.deferred[q];
+        // the cancel flag lives in host memory: a read crosses PCIe, so a warp
+        // looks at it once every kCancelPollTasks tasks, not per task
+        if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
+        const int t = (FAST || a.general_all) ? q : a.deferred[q];
         const dic_task T = a.tasks[t];
         if constexpr (FAST) {
             if (T.mode == DIC_INIT_AUTO_SEARCH) {
@@ -756,6 +761,448 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
     }
 }
 
+// ---------------------------------------------------------------------------
+// The fast pass: the common case of a solve (IC-GN with whole-subset
+// iterations only), one warp per subset and one warp per block, so that
+// shared memory alone sets the occupancy. Per task the warp stages its
+// reference subset in shared memory already normalised ((I - mean) / std and
+// the gradients / std, the products the iterations use), so the iterations
+// read only shared memory: the reference subset, the TMA tile of the
+// deformed image and the sampled values. Validity and Ghost Wall flags are
+// per-lane bit masks (pixel lane + 32k is bit k), the tile state is
+// warp-uniform registers. Arithmetic and summation order are those of
+// solve_kernel, so both passes give the same bits.
+//
+// Shared memory per warp: the TMA barrier at 0, the step matrix (36 doubles)
+// at 64, the tile at off_tile, then vals[n], rn[n], g0[n], g1[n].
+constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets go to the general pass
+
+struct FastLayout {
+    int off_tile, off_vals, off_rn, off_g0, off_g1;
+    int bytes;  // per warp, a multiple of 128
+};
+
+FastLayout fast_layout(int n, int tw, int th) {
+    FastLayout L;
+    L.off_tile = 384;
+    int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
+    const int arr = (n * 4 + 15) & ~15;
+    L.off_vals = p;
+    p += arr;
+    L.off_rn = p;
+    p += arr;
+    L.off_g0 = p;
+    p += arr;
+    L.off_g1 = p;
+    p += arr;
+    L.bytes = (p + 127) & ~127;
+    return L;
+}
+
+// Sample one pixel of the warped subset (sample_warped_subset,
+// optimization_engine.cpp:191-269): the value, and whether it lies inside
+// the guard. Loads only.
+template <bool SIX>
+__device__ __forceinline__ float fast_sample(const float* __restrict__ tile, const float* __restrict__ defI, int tw,
+                                             int th, int pitch, int tx0, int ty0, bool tile_ok, int cx, int cy,
+                                             float lo_x, float hi_x, float lo_y, float hi_y, const float W[6], float ox,
+                                             float oy, bool& inside) {
+    const int lo_tap = SIX ? 2 : 1, hi_tap = SIX ? 3 : 2;
+    const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
+    const float fy = __fmaf_rn(W[3], ox, __fmaf_rn(W[4], oy, W[5]));
+    const float rx = fx + 0.5f, ry = fy + 0.5f;
+    inside = rx >= lo_x && rx < hi_x && ry >= lo_y && ry < hi_y;
+    if (!inside) return 0.0f;
+    const float flx = floorf(fx), fly = floorf(fy);
+    const int xi = cx + (int)flx, yi = cy + (int)fly;
+    const int lx = xi - tx0, ly = yi - ty0;
+    if (tile_ok && lx >= lo_tap && lx + hi_tap < tw && ly >= lo_tap && ly + hi_tap < th)
+        return SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly) : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
+    return SIX ? interp6(defI, pitch, xi, yi, fx - flx, fy - fly) : interp4(defI, pitch, xi, yi, fx - flx, fy - fly);
+}
+
+template <bool SIX>
+__global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
+                                                  const FastLayout L) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    uint64_t* const bar = reinterpret_cast<uint64_t*>(smem);
+    double* const Hr = reinterpret_cast<double*>(smem + 64);
+    float* const tile = reinterpret_cast<float*>(smem + L.off_tile);
+    float* const vals = reinterpret_cast<float*>(smem + L.off_vals);
+    float* const srn = reinterpret_cast<float*>(smem + L.off_rn);
+    float* const sg0 = reinterpret_cast<float*>(smem + L.off_g0);
+    float* const sg1 = reinterpret_cast<float*>(smem + L.off_g1);
+    if (lane == 0) mbar_init(bar, 1);
+    fence_proxy_async_smem();
+    __syncwarp();
+
+    const int n = a.n, dim = a.dim, half = a.half, pitch = a.pitch, tw = a.tile_w, th = a.tile_h;
+    const int K = (n + 31) >> 5;  // pixels per lane
+    const int q = 32 / dim, r = 32 - q * dim;
+    const int row0 = lane / dim, col0 = lane - row0 * dim;
+    const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
+    const float* const refI = a.refI;
+    const float* const refGx = a.refGx;
+    const float* const refGy = a.refGy;
+    const float* const defI = a.defI;
+    int* const n_deferred = a.queue + 2;
+    int* const deferred = a.deferred;
+
+    // warp-uniform TMA tile state
+    int tx0 = 0, ty0 = 0;
+    bool tile_ok = false, tile_on = tw > 0;
+    unsigned phase = 0;
+
+    int polled = 0;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(a.queue, 1);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= ntasks) break;
+        // the cancel flag lives in host memory: a read crosses PCIe, so a warp
+        // looks at it once every kCancelPollTasks tasks, not per task
+        if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
+        const dic_task T = a.tasks[t];
+        if (T.mode == DIC_INIT_AUTO_SEARCH || K > kFastMaxPerLane) {
+            if (lane == 0) deferred[atomicAdd(n_deferred, 1)] = t;
+            __syncwarp();
+            continue;
+        }
+        dic_result out;
+        out.u = out.v = out.ux = out.uy = out.vx = out.vy = 0.0f;
+        out.score = 0.0f;
+        out.status = out.iters = out.trigger_iters = out.invalid_ref = out.flags = 0;
+        const bool dim_ok = dim >= 3 && (dim & 1) && dim * dim <= a.max_n;
+        const bool on_img = T.cx - half >= 0 && T.cx + half < a.W && T.cy - half >= 0 && T.cy + half < a.H;
+        if (!dim_ok || !on_img || !a.pool_valid[T.node]) {
+            if (lane == 0) a.results[t] = out;
+            continue;
+        }
+        const int cx = T.cx, cy = T.cy;
+        const float2 ms = a.pool_ms[T.node];
+        const float mref = ms.x, iref = 1.0f / ms.y;
+        // the whole-subset step matrix (optimization_engine.cpp:302-315), from the pool
+        {
+            const double* Hs21 = a.pool_Hs + (size_t)T.node * 21;
+            for (int k = lane; k < 36; k += 32) {
+                const int rr = k / 6, cc = k % 6;
+                Hr[k] = Hs21[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
+            }
+        }
+        // stage the reference subset, normalised; Ghost Wall flags and count
+        const int ref_base = (cy - half) * pitch + (cx - half);
+        uint64_t refok = 0;
+        int ghost = 0;
+        {
+            int row = row0, col = col0;
+#pragma unroll 4
+            for (int k = 0; k < K; ++k) {
+                const int i = lane + 32 * k;
+                if (i < n) {
+                    const int idx = ref_base + row * pitch + col;
+                    const float I = __ldg(refI + idx);
+                    const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
+                    if (I < kGhost)
+                        ++ghost;
+                    else
+                        refok |= 1ull << k;
+                    srn[i] = (I - mref) * iref;
+                    sg0[i] = gx * iref;
+                    sg1[i] = gy * iref;
+                }
+                col += r;
+                row += q;
+                if (col >= dim) {
+                    col -= dim;
+                    ++row;
+                }
+            }
+        }
+        ghost = wsum(ghost);
+        __syncwarp();
+
+        // calculate_deformation (optimization_engine.cpp:55-118) -> solve_icgn (:272-465)
+        const float lo_x = (float)(4 - cx), hi_x = (float)(a.W - 4 - cx);
+        const float lo_y = (float)(4 - cy), hi_y = (float)(a.H - 4 - cy);
+        float W[6] = {1.0f + T.g[2], T.g[3], T.g[0], T.g[4], 1.0f + T.g[5], T.g[1]};
+        float final_score = 1.0f;
+        Res res;
+        bool defer = false;
+        for (int iter = 0;; ++iter) {
+            if (iter == kIcgnMaxIter) {
+                res = res_from(W, 1, final_score, kIcgnMaxIter);
+                break;
+            }
+            // the tile must cover every sample support of the warped subset
+            if (tile_on) {
+                const float h = (float)half;
+                float mnx = 0.0f, mxx = 0.0f, mny = 0.0f, mxy = 0.0f;
+                bool in_range = true;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float ox = (k & 1) ? h : -h, oy = (k & 2) ? h : -h;
+                    const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
+                    const float fy = __fmaf_rn(W[3], ox, __fmaf_rn(W[4], oy, W[5]));
+                    in_range = in_range && fx > -1e6f && fx < 1e6f && fy > -1e6f && fy < 1e6f;
+                    mnx = k ? fminf(mnx, fx) : fx;
+                    mxx = k ? fmaxf(mxx, fx) : fx;
+                    mny = k ? fminf(mny, fy) : fy;
+                    mxy = k ? fmaxf(mxy, fy) : fy;
+                }
+                if (!in_range) {
+                    tile_ok = false;
+                } else {
+                    const int lo_tap = SIX ? 3 : 2, hi_tap = SIX ? 4 : 3;
+                    const int x_lo = cx + (int)floorf(mnx) - lo_tap, x_hi = cx + (int)floorf(mxx) + hi_tap;
+                    const int y_lo = cy + (int)floorf(mny) - lo_tap, y_hi = cy + (int)floorf(mxy) + hi_tap;
+                    if (!(tile_ok && x_lo >= tx0 && x_hi < tx0 + tw && y_lo >= ty0 && y_hi < ty0 + th)) {
+                        const int need_w = x_hi - x_lo + 1, need_h = y_hi - y_lo + 1;
+                        if (need_w + 3 > tw || need_h > th) {
+                            tile_ok = false;
+                        } else {
+                            // centre the support, x start on a 16-byte boundary (a multiple of 4)
+                            int nx = x_lo - (tw - 3 - need_w) / 2;
+                            nx = nx >= 0 ? (nx & ~3) : -((-nx + 3) & ~3);
+                            const int ny = y_lo - (th - need_h) / 2;
+                            __syncwarp();  // every lane is done with the old tile
+                            if (lane == 0) {
+                                fence_proxy_async_smem();
+                                mbar_arrive_expect_tx(bar, (uint32_t)(tw * th * 4));
+                                tma_load_2d(tile, &tmap, nx, ny, bar);
+                            }
+                            const bool done = __all_sync(kFull, mbar_wait_bounded(bar, phase, 1 << 22));
+                            phase ^= 1u;
+                            if (done) {
+                                tx0 = nx;
+                                ty0 = ny;
+                                tile_ok = true;
+                            } else {
+                                // a copy that never completed: stop staging for this warp
+                                tile_ok = false;
+                                tile_on = false;
+                                if (lane == 0 && a.err) atomicExch(a.err, 1);
+                            }
+                        }
+                    }
+                }
+            }
+            // pass 1: sample, four pixels' loads before their stores
+            float part = 0.0f;
+            int cnt = 0;
+            uint64_t valid = 0;
+            {
+                int row = row0, col = col0;
+                for (int k0 = 0; k0 < K; k0 += 4) {
+                    float v[4];
+                    int ii[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + u;
+                        ii[u] = lane + 32 * k;
+                        v[u] = 0.0f;
+                        if (k < K && ii[u] < n) {
+                            bool inside;
+                            v[u] = fast_sample<SIX>(tile, defI, tw, th, pitch, tx0, ty0, tile_ok, cx, cy, lo_x, hi_x,
+                                                    lo_y, hi_y, W, (float)(col - half), (float)(row - half), inside);
+                            if (inside && ((refok >> k) & 1ull)) {
+                                valid |= 1ull << k;
+                                part = part + v[u];
+                                ++cnt;
+                            }
+                        }
+                        col += r;
+                        row += q;
+                        if (col >= dim) {
+                            col -= dim;
+                            ++row;
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
+                }
+            }
+            __syncwarp();
+            const float sum = wsum(part);
+            cnt = wsum(cnt);
+            if (cnt < a.min_valid) {
+                res = res_from(W, 1, 2.0f, iter);
+                break;
+            }
+            if (cnt != n) {  // a masked iteration: the general pass solves this task
+                defer = true;
+                break;
+            }
+            const float mean = sum / (float)cnt;
+            float sq = 0.0f;
+#pragma unroll 4
+            for (int k = 0; k < K; ++k) {
+                if (!((valid >> k) & 1ull)) continue;
+                const float d = vals[lane + 32 * k] - mean;
+                sq = __fmaf_rn(d, d, sq);
+            }
+            float sdev = sqrtf(wsum(sq) / (float)cnt);
+            if (sdev < 1e-5f) sdev = 1.0f;
+            const float inv = 1.0f / sdev;
+
+            // pass 3: ZNSSD residual and steepest-descent 6-vector
+            float ep = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f, gp3 = 0.0f, gp4 = 0.0f, gp5 = 0.0f;
+            {
+                int row = row0, col = col0;
+#pragma unroll 4
+                for (int k = 0; k < K; ++k) {
+                    if ((valid >> k) & 1ull) {
+                        const int i = lane + 32 * k;
+                        const float rn = srn[i], g0 = sg0[i], g1 = sg1[i];
+                        const float fx = (float)(col - half), fy = (float)(row - half);
+                        const float nd = (vals[i] - mean) * inv;
+                        const float diff = rn - nd;
+                        ep = __fmaf_rn(diff, diff, ep);
+                        gp0 = __fmaf_rn(g0, diff, gp0);
+                        gp1 = __fmaf_rn(g1, diff, gp1);
+                        gp2 = __fmaf_rn(g0 * fx, diff, gp2);
+                        gp3 = __fmaf_rn(g0 * fy, diff, gp3);
+                        gp4 = __fmaf_rn(g1 * fx, diff, gp4);
+                        gp5 = __fmaf_rn(g1 * fy, diff, gp5);
+                    }
+                    col += r;
+                    row += q;
+                    if (col >= dim) {
+                        col -= dim;
+                        ++row;
+                    }
+                }
+            }
+            const float err = wsum(ep);
+            const float g[6] = {wsum(gp0), wsum(gp1), wsum(gp2), wsum(gp3), wsum(gp4), wsum(gp5)};
+            final_score = err / (float)cnt;
+
+            float dpl = 0.0f;
+            if (lane < 6) {
+                double acc = 0.0;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) acc = __fma_rn(Hr[lane * 6 + k], (double)g[k], acc);
+                dpl = (float)(-acc);
+            }
+            float dp[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) dp[k] = __shfl_sync(kFull, dpl, k);
+
+            const float a00 = 1.0f + dp[2], a01 = dp[3], a10 = dp[4], a11 = 1.0f + dp[5];
+            const float det = a00 * a11 - a01 * a10;
+            bool fin = true;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) fin = fin && finite_f(dp[k]);
+            if (!fin || !(fabsf(det) > 1e-6f)) {
+                res = res_from(W, 1, 2.0f, iter + 1);
+                break;
+            }
+            const float id = 1.0f / det;
+            const float i00 = a11 * id, i01 = -a01 * id, i10 = -a10 * id, i11 = a00 * id;
+            const float i02 = -(i00 * dp[0] + i01 * dp[1]);
+            const float i12 = -(i10 * dp[0] + i11 * dp[1]);
+            float Wn[6];
+            Wn[0] = W[0] * i00 + W[1] * i10;
+            Wn[1] = W[0] * i01 + W[1] * i11;
+            Wn[2] = (W[0] * i02 + W[1] * i12) + W[2];
+            Wn[3] = W[3] * i00 + W[4] * i10;
+            Wn[4] = W[3] * i01 + W[4] * i11;
+            Wn[5] = (W[3] * i02 + W[4] * i12) + W[5];
+            bool wfin = true;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) wfin = wfin && finite_f(Wn[k]);
+            if (!wfin) {
+                res = res_from(W, 1, 2.0f, iter + 1);
+                break;
+            }
+#pragma unroll
+            for (int k = 0; k < 6; ++k) W[k] = Wn[k];
+
+            float nn = dp[0] * dp[0];
+#pragma unroll
+            for (int k = 1; k < 6; ++k) nn = nn + dp[k] * dp[k];
+            if (sqrtf(nn) < 0.001f) {
+                // texture check on the raw reference gradients (optimization_engine.cpp:435-461)
+                float sx = 0.0f, sy = 0.0f;
+                int row = row0, col = col0;
+                for (int k = 0; k < K; ++k) {
+                    if ((valid >> k) & 1ull) {
+                        const int idx = ref_base + row * pitch + col;
+                        const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
+                        sx = __fmaf_rn(gx, gx, sx);
+                        sy = __fmaf_rn(gy, gy, sy);
+                    }
+                    col += r;
+                    row += q;
+                    if (col >= dim) {
+                        col -= dim;
+                        ++row;
+                    }
+                }
+                const float tx = wsum(sx), ty = wsum(sy);
+                const float sg = ty < tx ? ty : tx;
+                if (sg <= 0.0f || !finite_f(final_score))
+                    res = res_from(W, 1, 2.0f, iter + 1);
+                else
+                    res = res_from(W, 0, final_score, iter + 1);
+                break;
+            }
+        }
+        // a NO_SEARCH task that would take the Simplex rescue goes to the general pass
+        if (!defer && T.mode == DIC_INIT_NO_SEARCH && (res.status != 0 || res.score > kCorrSimplexTrigger))
+            defer = true;
+        if (defer) {
+            if (lane == 0) deferred[atomicAdd(n_deferred, 1)] = t;
+            __syncwarp();
+            continue;
+        }
+        if ((float)ghost / (float)(dim * dim) > kGhostRejectFraction) {
+            res.score = 2.0f;
+            res.status = 1;
+        }
+        if (lane == 0) {
+            out.u = res.u; out.v = res.v; out.ux = res.ux; out.uy = res.uy; out.vx = res.vx; out.vy = res.vy;
+            out.score = res.score;
+            out.status = res.status;
+            out.iters = res.iters;
+            out.trigger_iters = res.iters;
+            out.invalid_ref = ghost;
+            out.flags = DIC_RES_INITIALIZED;
+            a.results[t] = out;
+        }
+        __syncwarp();
+    }
+}
+
+constexpr int kFastMaxSmem = 227 * 1024;
+
+// The fast pass (one warp per block, as many blocks as fit on the device at
+// once, persistent) and then the general pass over what it handed on.
+template <bool SIX>
+cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const FastLayout& FL, bool fast_ok,
+                          int grid_blocks, size_t smem, cudaStream_t st) {
+    cudaError_t e;
+    if (fast_ok) {
+        e = cudaFuncSetAttribute(fast_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, FL.bytes);
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 0, per_sm = 0;
+        e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fast_kernel<SIX>, 32, FL.bytes);
+        if (e != cudaSuccess) return e;
+        long blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+        if (blocks > a.n_tasks) blocks = a.n_tasks > 0 ? a.n_tasks : 1;
+        fast_kernel<SIX><<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
+    }
+    e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    solve_kernel<SIX, false><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
+    return cudaGetLastError();
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static bool tried = false;
@@ -817,22 +1264,13 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     // queue[0]: fast pass, queue[1]: general pass, queue[2]: deferred count
     cudaError_t e = cudaMemsetAsync(a.queue, 0, 3 * sizeof(int), st);
     if (e != cudaSuccess) return e;
-    if (six) {
-        e = cudaFuncSetAttribute(solve_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(solve_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        solve_kernel<true, true><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
-        solve_kernel<true, false><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
-    } else {
-        e = cudaFuncSetAttribute(solve_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(solve_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        solve_kernel<false, true><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
-        solve_kernel<false, false><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
-    }
-    return cudaGetLastError();
+    // the fast pass takes subsets up to kFastMaxPerLane pixels per lane whose
+    // shared memory fits one block; otherwise the general pass takes every task
+    const FastLayout FL = fast_layout(a.n, tw, th);
+    const bool fast_ok = ((a.n + 31) >> 5) <= kFastMaxPerLane && FL.bytes <= kFastMaxSmem;
+    a.general_all = fast_ok ? 0 : 1;
+    return six ? launch_passes<true>(tmap, a, FL, fast_ok, grid_blocks, smem, st)
+               : launch_passes<false>(tmap, a, FL, fast_ok, grid_blocks, smem, st);
 }
 
 }  // namespace dic

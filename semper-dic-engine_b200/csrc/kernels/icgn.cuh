@@ -36,6 +36,7 @@ struct SolveArgs {
     // set by launch_solve from dim and the shared-memory layout
     int half, n, min_valid;
     int off_tile, off_vals, off_valid, off_refok;
+    int general_all;  // set by launch_solve: the general pass takes every task (no fast pass)
 };
 
 struct SmemLayout {
