@@ -244,6 +244,79 @@ struct Engine::Impl {
     int sm_count = 0;
     cudaEvent_t ev[10];
 
+    // Path B keeps two rounds in flight (full_field_path_b.cpp:148-412). Each
+    // in-flight round has its own slot: device buffers, scratch, a stream and
+    // pinned host staging, so the second round's solves run on the device
+    // while the first round is committed on the host.
+    struct Slot {
+        DevBuf<dic_task> tasks;
+        DevBuf<dic_result> results;
+        DevBuf<int> q, deferred;
+        dic_task* h_tasks = nullptr;  // pinned
+        dic_result* h_results = nullptr;
+        size_t h_n = 0, n = 0;
+        cudaStream_t s = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    Slot slots[2];
+
+    ~Impl() {
+        for (Slot& S : slots) {
+            if (S.h_tasks) cudaFreeHost(S.h_tasks);
+            if (S.h_results) cudaFreeHost(S.h_results);
+            if (S.done) cudaEventDestroy(S.done);
+            if (S.s) cudaStreamDestroy(S.s);
+        }
+    }
+
+    // Enqueue one round's solves on slot k, after the work already on the
+    // engine stream (event `after`); results land in the slot's pinned buffer.
+    void launch_round(int k, const std::vector<dic_task>& tk, const Params& p, cudaEvent_t after) {
+        Slot& S = slots[k];
+        if (!S.s) {
+            check(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking), "slot stream");
+            check(cudaEventCreateWithFlags(&S.done, cudaEventDisableTiming), "slot event");
+            S.q.ensure(8);
+        }
+        S.n = tk.size();
+        check(cudaStreamWaitEvent(S.s, after, 0), "slot wait");
+        if (S.n > 0) {
+            if (S.h_n < S.n) {
+                if (S.h_tasks) cudaFreeHost(S.h_tasks);
+                if (S.h_results) cudaFreeHost(S.h_results);
+                S.h_tasks = nullptr;
+                S.h_results = nullptr;
+                S.h_n = 0;
+                check(cudaMallocHost(&S.h_tasks, S.n * sizeof(dic_task)), "pinned tasks");
+                check(cudaMallocHost(&S.h_results, S.n * sizeof(dic_result)), "pinned results");
+                S.h_n = S.n;
+            }
+            S.tasks.ensure(std::max(S.tasks.n, S.n));
+            S.results.ensure(std::max(S.results.n, S.n));
+            S.deferred.ensure(std::max(S.deferred.n, S.n));
+            std::memcpy(S.h_tasks, tk.data(), S.n * sizeof(dic_task));
+            check(cudaMemcpyAsync(S.tasks.p, S.h_tasks, S.n * sizeof(dic_task), cudaMemcpyHostToDevice, S.s),
+                  "H2D round");
+            dic::SolveArgs a = solve_args(p.subset_size, p.six);
+            a.tasks = S.tasks.p;
+            a.n_tasks = (int)S.n;
+            a.n_tasks_dev = nullptr;
+            a.results = S.results.p;
+            a.queue = S.q.p;
+            a.deferred = S.deferred.p;
+            launched(2, dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)S.n), S.s), "round solve");
+            check(cudaMemcpyAsync(S.h_results, S.results.p, S.n * sizeof(dic_result), cudaMemcpyDeviceToHost, S.s),
+                  "D2H round");
+        }
+        check(cudaEventRecord(S.done, S.s), "slot record");
+    }
+
+    const dic_result* wait_round(int k) {
+        check(cudaEventSynchronize(slots[k].done), "slot sync");
+        poll_cancel();
+        return slots[k].h_results;
+    }
+
     dic::FieldGrid field() {
         return dic::FieldGrid{fu.p, fv.p, fux.p, fuy.p, fvx.p, fvy.p, fcorr.p, fsolved.p, fiters.p};
     }
@@ -1039,13 +1112,24 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 rounds.push_back(std::move(r));
                 return true;
             };
-            while (rounds.size() < 2 && claim()) {}
+            // Round k runs on slot k % 2; its solves start as soon as it is
+            // claimed, so two rounds run on the device at once.
+            check(cudaEventRecord(ev[9], st), "event");
+            int launched_rounds = 0, done_rounds = 0;
+            auto claim_launch = [&]() -> bool {
+                if (!claim()) return false;
+                launch_round(launched_rounds % 2, rounds.back(), params, ev[9]);
+                ++launched_rounds;
+                return true;
+            };
+            while (rounds.size() < 2 && claim_launch()) {}
             while (!rounds.empty()) {
                 const std::vector<dic_task> r = std::move(rounds.front());
                 rounds.pop_front();
-                const std::vector<dic_result> rs = solve_batch(r, params);
+                const dic_result* rs = wait_round(done_rounds % 2);
+                ++done_rounds;
                 for (size_t k = 0; k < r.size(); ++k) commit(r[k], rs[k], true);
-                while (rounds.size() < 2 && claim()) {}
+                while (rounds.size() < 2 && claim_launch()) {}
             }
             if (!recs.empty()) {
                 scat.ensure(std::max(scat.n, recs.size()));
@@ -1057,6 +1141,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         }
         check(cudaEventRecord(ev[7], st), "event");
         const double ms_b = ms_since(t_b);
+        E.times_.path_b = ms_b;
         poll_cancel();
 
         if (capture) {

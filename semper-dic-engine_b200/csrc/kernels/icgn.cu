@@ -29,13 +29,9 @@
 #include "icgn.cuh"
 #include "tma.cuh"
 
-// Unroll factor of the per-pixel loops and the occupancy target of the solve
-// kernel (blocks of kSolveThreads per SM): chosen by measurement on B200.
+// Unroll factor of the general pass's per-pixel loops.
 #ifndef DIC_PIXEL_UNROLL
 #define DIC_PIXEL_UNROLL 2
-#endif
-#ifndef DIC_SOLVE_MIN_BLOCKS
-#define DIC_SOLVE_MIN_BLOCKS 4
 #endif
 
 namespace dic {
@@ -611,7 +607,7 @@ __device__ __noinline__ float2 coarse(Ctx c, float gu, float gv) {
 // search), every other task appended to the deferred list. General: the
 // deferred tasks, with every path.
 template <bool SIX, bool FAST>
-__global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
+__global__ void __launch_bounds__(32, 1)
     solve_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -765,16 +761,16 @@ __global__ void __launch_bounds__(kSolveThreads, DIC_SOLVE_MIN_BLOCKS)
 // The fast pass: the common case of a solve (IC-GN with whole-subset
 // iterations only), one warp per subset and one warp per block, so that
 // shared memory alone sets the occupancy. Per task the warp stages its
-// reference subset in shared memory already normalised ((I - mean) / std and
-// the gradients / std, the products the iterations use), so the iterations
-// read only shared memory: the reference subset, the TMA tile of the
-// deformed image and the sampled values. Validity and Ghost Wall flags are
+// reference subset in shared memory ((I - mean) / std, and the raw gradients,
+// which the texture check needs as they are), so the iterations read only
+// shared memory: the reference subset, the TMA tile of the deformed image and
+// the sampled values. Validity and Ghost Wall flags are
 // per-lane bit masks (pixel lane + 32k is bit k), the tile state is
 // warp-uniform registers. Arithmetic and summation order are those of
 // solve_kernel, so both passes give the same bits.
 //
 // Shared memory per warp: the TMA barrier at 0, the step matrix (36 doubles)
-// at 64, the tile at off_tile, then vals[n], rn[n], g0[n], g1[n].
+// at 64, the tile at off_tile, then vals[n], rn[n], gx[n], gy[n].
 constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets go to the general pass
 
 struct FastLayout {
@@ -831,8 +827,8 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
     float* const tile = reinterpret_cast<float*>(smem + L.off_tile);
     float* const vals = reinterpret_cast<float*>(smem + L.off_vals);
     float* const srn = reinterpret_cast<float*>(smem + L.off_rn);
-    float* const sg0 = reinterpret_cast<float*>(smem + L.off_g0);
-    float* const sg1 = reinterpret_cast<float*>(smem + L.off_g1);
+    float* const sgx = reinterpret_cast<float*>(smem + L.off_g0);
+    float* const sgy = reinterpret_cast<float*>(smem + L.off_g1);
     if (lane == 0) mbar_init(bar, 1);
     fence_proxy_async_smem();
     __syncwarp();
@@ -908,8 +904,8 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
                     else
                         refok |= 1ull << k;
                     srn[i] = (I - mref) * iref;
-                    sg0[i] = gx * iref;
-                    sg1[i] = gy * iref;
+                    sgx[i] = gx;
+                    sgy[i] = gy;
                 }
                 col += r;
                 row += q;
@@ -1054,7 +1050,7 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
                 for (int k = 0; k < K; ++k) {
                     if ((valid >> k) & 1ull) {
                         const int i = lane + 32 * k;
-                        const float rn = srn[i], g0 = sg0[i], g1 = sg1[i];
+                        const float rn = srn[i], g0 = sgx[i] * iref, g1 = sgy[i] * iref;
                         const float fx = (float)(col - half), fy = (float)(row - half);
                         const float nd = (vals[i] - mean) * inv;
                         const float diff = rn - nd;
@@ -1125,19 +1121,13 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
             if (sqrtf(nn) < 0.001f) {
                 // texture check on the raw reference gradients (optimization_engine.cpp:435-461)
                 float sx = 0.0f, sy = 0.0f;
-                int row = row0, col = col0;
+#pragma unroll 4
                 for (int k = 0; k < K; ++k) {
                     if ((valid >> k) & 1ull) {
-                        const int idx = ref_base + row * pitch + col;
-                        const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
+                        const int i = lane + 32 * k;
+                        const float gx = sgx[i], gy = sgy[i];
                         sx = __fmaf_rn(gx, gx, sx);
                         sy = __fmaf_rn(gy, gy, sy);
-                    }
-                    col += r;
-                    row += q;
-                    if (col >= dim) {
-                        col -= dim;
-                        ++row;
                     }
                 }
                 const float tx = wsum(sx), ty = wsum(sy);
@@ -1197,9 +1187,22 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Fas
         if (blocks > a.n_tasks) blocks = a.n_tasks > 0 ? a.n_tasks : 1;
         fast_kernel<SIX><<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
     }
+    // the general pass: one warp per block with the whole register file (its
+    // rare paths inline without spilling), as many blocks as fit at once
     e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    solve_kernel<SIX, false><<<grid_blocks, kSolveThreads, smem, st>>>(tmap, a);
+    int dev = 0, sms = 0, per_sm = 0;
+    e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_kernel<SIX, false>, 32, smem);
+    if (e != cudaSuccess) return e;
+    long blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    // the caller's hint counts units of kSolveThreads / 32 subsets
+    if (grid_blocks > 0 && blocks > (long)grid_blocks * (kSolveThreads / 32)) blocks = (long)grid_blocks * (kSolveThreads / 32);
+    if (blocks > a.n_tasks) blocks = a.n_tasks > 0 ? a.n_tasks : 1;
+    solve_kernel<SIX, false><<<(unsigned)blocks, 32, smem, st>>>(tmap, a);
     return cudaGetLastError();
 }
 
@@ -1260,7 +1263,7 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     a.off_vals = (int)L.off_vals;
     a.off_valid = (int)L.off_valid;
     a.off_refok = (int)L.off_refok;
-    const size_t smem = kArgsBytes + a.smem_per_warp * (kSolveThreads / 32);
+    const size_t smem = kArgsBytes + a.smem_per_warp;
     // queue[0]: fast pass, queue[1]: general pass, queue[2]: deferred count
     cudaError_t e = cudaMemsetAsync(a.queue, 0, 3 * sizeof(int), st);
     if (e != cudaSuccess) return e;

@@ -8,7 +8,7 @@
 
 namespace dic {
 
-constexpr int kSolveThreads = 128;  // 4 warps per block, one subset per warp
+constexpr int kSolveThreads = 128;  // unit of the `blocks` grid-size hint: 4 subsets per unit
 
 struct SolveArgs {
     const float* refI;   // reference intensities (Ghost Wall stamped), W x H
