@@ -758,291 +758,317 @@ __global__ void __launch_bounds__(32, 1)
 }
 
 // ---------------------------------------------------------------------------
-// The fast pass: the common case of a solve (IC-GN with whole-subset
-// iterations only), one warp per subset and one warp per block, so that
+// The staged solvers: one warp per subset and one warp per block, so that
 // shared memory alone sets the occupancy. Per task the warp stages its
 // reference subset in shared memory ((I - mean) / std, and the raw gradients,
 // which the texture check needs as they are), so the iterations read only
 // shared memory: the reference subset, the TMA tile of the deformed image and
-// the sampled values. Validity and Ghost Wall flags are
-// per-lane bit masks (pixel lane + 32k is bit k), the tile state is
-// warp-uniform registers. Arithmetic and summation order are those of
-// solve_kernel, so both passes give the same bits.
+// the sampled values. Validity and Ghost Wall flags are per-lane bit masks
+// (pixel lane + 32k is bit k); the tile state is warp-uniform registers.
+// Arithmetic and summation order are those of solve_kernel (and of the CPU
+// restatement), so every kernel gives the same bits.
 //
-// Shared memory per warp: the TMA barrier at 0, the step matrix (36 doubles)
-// at 64, the tile at off_tile, then vals[n], rn[n], gx[n], gy[n].
-constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets go to the general pass
+// Two kernels share this code. The fast pass runs every task's common case
+// (IC-GN with whole-subset iterations) and hands every other task (AUTO
+// mode, a masked iteration, a NO_SEARCH rescue) to a list; the rescue pass
+// runs those tasks from the start with every path.
+//
+// Shared memory per warp: the TMA barrier at 0, the whole-subset step matrix
+// (36 doubles) at 64, the masked-iteration step matrix at 352, the tile at
+// off_tile, then vals[n], rn[n], gx[n], gy[n].
+constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets go to solve_kernel
+constexpr int kFastMaxSmem = 227 * 1024;
 
-struct FastLayout {
-    int off_tile, off_vals, off_rn, off_g0, off_g1;
+struct StagedLayout {
+    int off_tile, off_vals, off_rn, off_gx, off_gy;
     int bytes;  // per warp, a multiple of 128
 };
 
-FastLayout fast_layout(int n, int tw, int th) {
-    FastLayout L;
-    L.off_tile = 384;
+StagedLayout staged_layout(int n, int tw, int th) {
+    StagedLayout L;
+    L.off_tile = 640;
     int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
     const int arr = (n * 4 + 15) & ~15;
     L.off_vals = p;
     p += arr;
     L.off_rn = p;
     p += arr;
-    L.off_g0 = p;
+    L.off_gx = p;
     p += arr;
-    L.off_g1 = p;
+    L.off_gy = p;
     p += arr;
     L.bytes = (p + 127) & ~127;
     return L;
 }
 
-// Sample one pixel of the warped subset (sample_warped_subset,
-// optimization_engine.cpp:191-269): the value, and whether it lies inside
-// the guard. Loads only.
 template <bool SIX>
-__device__ __forceinline__ float fast_sample(const float* __restrict__ tile, const float* __restrict__ defI, int tw,
-                                             int th, int pitch, int tx0, int ty0, bool tile_ok, int cx, int cy,
-                                             float lo_x, float hi_x, float lo_y, float hi_y, const float W[6], float ox,
-                                             float oy, bool& inside) {
-    const int lo_tap = SIX ? 2 : 1, hi_tap = SIX ? 3 : 2;
-    const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
-    const float fy = __fmaf_rn(W[3], ox, __fmaf_rn(W[4], oy, W[5]));
-    const float rx = fx + 0.5f, ry = fy + 0.5f;
-    inside = rx >= lo_x && rx < hi_x && ry >= lo_y && ry < hi_y;
-    if (!inside) return 0.0f;
-    const float flx = floorf(fx), fly = floorf(fy);
-    const int xi = cx + (int)flx, yi = cy + (int)fly;
-    const int lx = xi - tx0, ly = yi - ty0;
-    if (tile_ok && lx >= lo_tap && lx + hi_tap < tw && ly >= lo_tap && ly + hi_tap < th)
-        return SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly) : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
-    return SIX ? interp6(defI, pitch, xi, yi, fx - flx, fy - fly) : interp4(defI, pitch, xi, yi, fx - flx, fy - fly);
-}
+struct WarpSolver {
+    // this warp's shared memory
+    uint64_t* bar;
+    double* Hr;
+    double* Hm;
+    float* tile;
+    float* vals;
+    float* srn;
+    float* sgx;
+    float* sgy;
+    const CUtensorMap* tmap;
+    // launch constants
+    const float* refI;
+    const float* refGx;
+    const float* refGy;
+    const float* defI;
+    int* err;
+    int n, dim, half, pitch, tw, th, W, H, K, q, r, row0, col0, lane, min_valid, lm;
+    // the TMA tile (warp-uniform)
+    int tx0, ty0;
+    bool tile_ok, tile_on;
+    unsigned phase;
+    // the task
+    int cx, cy, ref_base, ghost;
+    float mref, iref, lo_x, hi_x, lo_y, hi_y;
+    uint64_t refok;
 
-template <bool SIX>
-__global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
-                                                  const FastLayout L) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    const int lane = threadIdx.x & 31;
-    uint64_t* const bar = reinterpret_cast<uint64_t*>(smem);
-    double* const Hr = reinterpret_cast<double*>(smem + 64);
-    float* const tile = reinterpret_cast<float*>(smem + L.off_tile);
-    float* const vals = reinterpret_cast<float*>(smem + L.off_vals);
-    float* const srn = reinterpret_cast<float*>(smem + L.off_rn);
-    float* const sgx = reinterpret_cast<float*>(smem + L.off_g0);
-    float* const sgy = reinterpret_cast<float*>(smem + L.off_g1);
-    if (lane == 0) mbar_init(bar, 1);
-    fence_proxy_async_smem();
-    __syncwarp();
-
-    const int n = a.n, dim = a.dim, half = a.half, pitch = a.pitch, tw = a.tile_w, th = a.tile_h;
-    const int K = (n + 31) >> 5;  // pixels per lane
-    const int q = 32 / dim, r = 32 - q * dim;
-    const int row0 = lane / dim, col0 = lane - row0 * dim;
-    const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
-    const float* const refI = a.refI;
-    const float* const refGx = a.refGx;
-    const float* const refGy = a.refGy;
-    const float* const defI = a.defI;
-    int* const n_deferred = a.queue + 2;
-    int* const deferred = a.deferred;
-
-    // warp-uniform TMA tile state
-    int tx0 = 0, ty0 = 0;
-    bool tile_ok = false, tile_on = tw > 0;
-    unsigned phase = 0;
-
-    int polled = 0;
-    for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(a.queue, 1);
-        t = __shfl_sync(kFull, t, 0);
-        if (t >= ntasks) break;
-        // the cancel flag lives in host memory: a read crosses PCIe, so a warp
-        // looks at it once every kCancelPollTasks tasks, not per task
-        if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
-        const dic_task T = a.tasks[t];
-        if (T.mode == DIC_INIT_AUTO_SEARCH || K > kFastMaxPerLane) {
-            if (lane == 0) deferred[atomicAdd(n_deferred, 1)] = t;
-            __syncwarp();
-            continue;
+    __device__ __forceinline__ void advance(int& row, int& col) const {
+        col += r;
+        row += q;
+        if (col >= dim) {
+            col -= dim;
+            ++row;
         }
-        dic_result out;
-        out.u = out.v = out.ux = out.uy = out.vx = out.vy = 0.0f;
-        out.score = 0.0f;
-        out.status = out.iters = out.trigger_iters = out.invalid_ref = out.flags = 0;
-        const bool dim_ok = dim >= 3 && (dim & 1) && dim * dim <= a.max_n;
-        const bool on_img = T.cx - half >= 0 && T.cx + half < a.W && T.cy - half >= 0 && T.cy + half < a.H;
-        if (!dim_ok || !on_img || !a.pool_valid[T.node]) {
-            if (lane == 0) a.results[t] = out;
-            continue;
-        }
-        const int cx = T.cx, cy = T.cy;
-        const float2 ms = a.pool_ms[T.node];
-        const float mref = ms.x, iref = 1.0f / ms.y;
+    }
+
+    // Per task: the step matrix from the pool, the reference subset staged
+    // and normalised, the Ghost Wall flags and count.
+    __device__ __forceinline__ void begin(const dic_task& T, float2 ms, const double* Hs21) {
+        cx = T.cx;
+        cy = T.cy;
+        mref = ms.x;
+        iref = 1.0f / ms.y;
+        lo_x = (float)(4 - cx);
+        hi_x = (float)(W - 4 - cx);
+        lo_y = (float)(4 - cy);
+        hi_y = (float)(H - 4 - cy);
         // the whole-subset step matrix (optimization_engine.cpp:302-315), from the pool
-        {
-            const double* Hs21 = a.pool_Hs + (size_t)T.node * 21;
-            for (int k = lane; k < 36; k += 32) {
-                const int rr = k / 6, cc = k % 6;
-                Hr[k] = Hs21[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
-            }
+        for (int k = lane; k < 36; k += 32) {
+            const int rr = k / 6, cc = k % 6;
+            Hr[k] = Hs21[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
         }
-        // stage the reference subset, normalised; Ghost Wall flags and count
-        const int ref_base = (cy - half) * pitch + (cx - half);
-        uint64_t refok = 0;
-        int ghost = 0;
-        {
-            int row = row0, col = col0;
+        ref_base = (cy - half) * pitch + (cx - half);
+        refok = 0;
+        int g = 0;
+        int row = row0, col = col0;
 #pragma unroll 4
-            for (int k = 0; k < K; ++k) {
-                const int i = lane + 32 * k;
-                if (i < n) {
-                    const int idx = ref_base + row * pitch + col;
-                    const float I = __ldg(refI + idx);
-                    const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
-                    if (I < kGhost)
-                        ++ghost;
-                    else
-                        refok |= 1ull << k;
-                    srn[i] = (I - mref) * iref;
-                    sgx[i] = gx;
-                    sgy[i] = gy;
+        for (int k = 0; k < K; ++k) {
+            const int i = lane + 32 * k;
+            if (i < n) {
+                const int idx = ref_base + row * pitch + col;
+                const float I = __ldg(refI + idx);
+                const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
+                if (I < kGhost)
+                    ++g;
+                else
+                    refok |= 1ull << k;
+                srn[i] = (I - mref) * iref;
+                sgx[i] = gx;
+                sgy[i] = gy;
+            }
+            advance(row, col);
+        }
+        ghost = wsum(g);
+        __syncwarp();
+    }
+
+    // The tile must cover every sample support of the warped subset: stage a
+    // new box with TMA when the warp has left the current one.
+    __device__ __forceinline__ void ensure_tile(const float Wp[6]) {
+        if (!tile_on) return;
+        const float h = (float)half;
+        float mnx = 0.0f, mxx = 0.0f, mny = 0.0f, mxy = 0.0f;
+        bool in_range = true;  // every corner finite and within 1e6 px (a NaN fails the comparisons)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const float ox = (k & 1) ? h : -h, oy = (k & 2) ? h : -h;
+            const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
+            const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
+            in_range = in_range && fx > -1e6f && fx < 1e6f && fy > -1e6f && fy < 1e6f;
+            mnx = k ? fminf(mnx, fx) : fx;
+            mxx = k ? fmaxf(mxx, fx) : fx;
+            mny = k ? fminf(mny, fy) : fy;
+            mxy = k ? fmaxf(mxy, fy) : fy;
+        }
+        if (!in_range) {
+            tile_ok = false;
+            return;
+        }
+        const int lo_tap = SIX ? 3 : 2, hi_tap = SIX ? 4 : 3;
+        const int x_lo = cx + (int)floorf(mnx) - lo_tap, x_hi = cx + (int)floorf(mxx) + hi_tap;
+        const int y_lo = cy + (int)floorf(mny) - lo_tap, y_hi = cy + (int)floorf(mxy) + hi_tap;
+        if (tile_ok && x_lo >= tx0 && x_hi < tx0 + tw && y_lo >= ty0 && y_hi < ty0 + th) return;
+        const int need_w = x_hi - x_lo + 1, need_h = y_hi - y_lo + 1;
+        if (need_w + 3 > tw || need_h > th) {
+            tile_ok = false;
+            return;
+        }
+        // centre the support, x start on a 16-byte boundary (a multiple of 4)
+        int nx = x_lo - (tw - 3 - need_w) / 2;
+        nx = nx >= 0 ? (nx & ~3) : -((-nx + 3) & ~3);
+        const int ny = y_lo - (th - need_h) / 2;
+        __syncwarp();  // every lane is done with the old tile
+        if (lane == 0) {
+            fence_proxy_async_smem();
+            mbar_arrive_expect_tx(bar, (uint32_t)(tw * th * 4));
+            tma_load_2d(tile, tmap, nx, ny, bar);
+        }
+        const bool done = __all_sync(kFull, mbar_wait_bounded(bar, phase, 1 << 22));
+        phase ^= 1u;
+        if (done) {
+            tx0 = nx;
+            ty0 = ny;
+            tile_ok = true;
+        } else {
+            // a copy that never completed: stop staging for this warp
+            tile_ok = false;
+            tile_on = false;
+            if (lane == 0 && err) atomicExch(err, 1);
+        }
+    }
+
+    // sample_warped_subset (optimization_engine.cpp:191-269): every pixel's
+    // value into vals, the valid ones (inside the guard, outside the Ghost
+    // Wall) flagged in `valid` and summed; returns their count. Four pixels'
+    // loads are issued before their stores.
+    __device__ __forceinline__ int sample(const float Wp[6], float& sum, uint64_t& valid) {
+        ensure_tile(Wp);
+        const int lo_tap = SIX ? 2 : 1, hi_tap = SIX ? 3 : 2;
+        float part = 0.0f;
+        int cnt = 0;
+        valid = 0;
+        int row = row0, col = col0;
+        for (int k0 = 0; k0 < K; k0 += 4) {
+            float v[4];
+            int ii[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u;
+                ii[u] = lane + 32 * k;
+                v[u] = 0.0f;
+                if (k < K && ii[u] < n) {
+                    const float ox = (float)(col - half), oy = (float)(row - half);
+                    const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
+                    const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
+                    const float rx = fx + 0.5f, ry = fy + 0.5f;
+                    if (rx >= lo_x && rx < hi_x && ry >= lo_y && ry < hi_y) {
+                        const float flx = floorf(fx), fly = floorf(fy);
+                        const int xi = cx + (int)flx, yi = cy + (int)fly;
+                        const int lx = xi - tx0, ly = yi - ty0;
+                        if (tile_ok && lx >= lo_tap && lx + hi_tap < tw && ly >= lo_tap && ly + hi_tap < th)
+                            v[u] = SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly)
+                                       : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
+                        else
+                            v[u] = SIX ? interp6(defI, pitch, xi, yi, fx - flx, fy - fly)
+                                       : interp4(defI, pitch, xi, yi, fx - flx, fy - fly);
+                        if ((refok >> k) & 1ull) {
+                            valid |= 1ull << k;
+                            part = part + v[u];
+                            ++cnt;
+                        }
+                    }
                 }
-                col += r;
-                row += q;
-                if (col >= dim) {
-                    col -= dim;
-                    ++row;
+                advance(row, col);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
+        }
+        __syncwarp();
+        sum = wsum(part);
+        return wsum(cnt);
+    }
+
+    __device__ __forceinline__ float sum_sq(float mean, uint64_t valid) const {
+        float sq = 0.0f;
+#pragma unroll 4
+        for (int k = 0; k < K; ++k) {
+            if (!((valid >> k) & 1ull)) continue;
+            const float d = vals[lane + 32 * k] - mean;
+            sq = __fmaf_rn(d, d, sq);
+        }
+        return wsum(sq);
+    }
+
+    // The masked iteration's own Hessian (optimization_engine.cpp:373-413),
+    // FP64, into Hm; false to reject.
+    __device__ __forceinline__ bool masked_step(uint64_t valid) {
+        double hp[21];
+#pragma unroll
+        for (int k = 0; k < 21; ++k) hp[k] = 0.0;
+        int row = row0, col = col0;
+        for (int k = 0; k < K; ++k) {
+            if ((valid >> k) & 1ull) {
+                const int i = lane + 32 * k;
+                const float g0 = sgx[i] * iref, g1 = sgy[i] * iref;
+                const float fx = (float)(col - half), fy = (float)(row - half);
+                const double s[6] = {(double)g0, (double)g1, (double)(g0 * fx), (double)(g0 * fy),
+                                     (double)(g1 * fx), (double)(g1 * fy)};
+                int m = 0;
+#pragma unroll
+                for (int aa = 0; aa < 6; ++aa)
+#pragma unroll
+                    for (int bb = aa; bb < 6; ++bb, ++m) hp[m] = __fma_rn(s[aa], s[bb], hp[m]);
+            }
+            advance(row, col);
+        }
+#pragma unroll
+        for (int k = 0; k < 21; ++k) hp[k] = wsum(hp[k]);
+        int ok = 0;
+        if (lane == 0) {
+            double Hd[6][6], Hi[6][6];
+            for (int aa = 0; aa < 6; ++aa)
+                for (int bb = aa; bb < 6; ++bb) {
+                    Hd[aa][bb] = hp[tri21(aa, bb)];
+                    Hd[bb][aa] = Hd[aa][bb];
+                }
+            if (cond2x2_ok(Hd)) {
+                if (lm) {
+                    Hd[0][0] += (double)kLmAlpha;
+                    Hd[1][1] += (double)kLmAlpha;
+                }
+                if (well_conditioned(Hd, half) && inverse6(Hd, Hi)) {
+                    for (int aa = 0; aa < 6; ++aa)
+                        for (int bb = 0; bb < 6; ++bb) Hm[aa * 6 + bb] = Hi[aa][bb];
+                    ok = 1;
                 }
             }
         }
-        ghost = wsum(ghost);
+        ok = __shfl_sync(kFull, ok, 0);
         __syncwarp();
+        return ok != 0;
+    }
 
-        // calculate_deformation (optimization_engine.cpp:55-118) -> solve_icgn (:272-465)
-        const float lo_x = (float)(4 - cx), hi_x = (float)(a.W - 4 - cx);
-        const float lo_y = (float)(4 - cy), hi_y = (float)(a.H - 4 - cy);
-        float W[6] = {1.0f + T.g[2], T.g[3], T.g[0], T.g[4], 1.0f + T.g[5], T.g[1]};
+    // solve_icgn (optimization_engine.cpp:272-465). With GENERAL false a
+    // masked iteration is not taken: `defer` is set instead.
+    template <bool GENERAL>
+    __device__ __forceinline__ Res icgn(const float st[6], bool& defer) {
+        float Wp[6] = {1.0f + st[2], st[3], st[0], st[4], 1.0f + st[5], st[1]};
         float final_score = 1.0f;
-        Res res;
-        bool defer = false;
-        for (int iter = 0;; ++iter) {
-            if (iter == kIcgnMaxIter) {
-                res = res_from(W, 1, final_score, kIcgnMaxIter);
-                break;
-            }
-            // the tile must cover every sample support of the warped subset
-            if (tile_on) {
-                const float h = (float)half;
-                float mnx = 0.0f, mxx = 0.0f, mny = 0.0f, mxy = 0.0f;
-                bool in_range = true;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float ox = (k & 1) ? h : -h, oy = (k & 2) ? h : -h;
-                    const float fx = __fmaf_rn(W[0], ox, __fmaf_rn(W[1], oy, W[2]));
-                    const float fy = __fmaf_rn(W[3], ox, __fmaf_rn(W[4], oy, W[5]));
-                    in_range = in_range && fx > -1e6f && fx < 1e6f && fy > -1e6f && fy < 1e6f;
-                    mnx = k ? fminf(mnx, fx) : fx;
-                    mxx = k ? fmaxf(mxx, fx) : fx;
-                    mny = k ? fminf(mny, fy) : fy;
-                    mxy = k ? fmaxf(mxy, fy) : fy;
+        for (int iter = 0; iter < kIcgnMaxIter; ++iter) {
+            float sum;
+            uint64_t valid;
+            const int cnt = sample(Wp, sum, valid);
+            if (cnt < min_valid) return res_from(Wp, 1, 2.0f, iter);
+            const bool full = cnt == n;
+            if constexpr (!GENERAL) {
+                if (!full) {
+                    defer = true;
+                    return res_from(Wp, 1, 2.0f, iter);
                 }
-                if (!in_range) {
-                    tile_ok = false;
-                } else {
-                    const int lo_tap = SIX ? 3 : 2, hi_tap = SIX ? 4 : 3;
-                    const int x_lo = cx + (int)floorf(mnx) - lo_tap, x_hi = cx + (int)floorf(mxx) + hi_tap;
-                    const int y_lo = cy + (int)floorf(mny) - lo_tap, y_hi = cy + (int)floorf(mxy) + hi_tap;
-                    if (!(tile_ok && x_lo >= tx0 && x_hi < tx0 + tw && y_lo >= ty0 && y_hi < ty0 + th)) {
-                        const int need_w = x_hi - x_lo + 1, need_h = y_hi - y_lo + 1;
-                        if (need_w + 3 > tw || need_h > th) {
-                            tile_ok = false;
-                        } else {
-                            // centre the support, x start on a 16-byte boundary (a multiple of 4)
-                            int nx = x_lo - (tw - 3 - need_w) / 2;
-                            nx = nx >= 0 ? (nx & ~3) : -((-nx + 3) & ~3);
-                            const int ny = y_lo - (th - need_h) / 2;
-                            __syncwarp();  // every lane is done with the old tile
-                            if (lane == 0) {
-                                fence_proxy_async_smem();
-                                mbar_arrive_expect_tx(bar, (uint32_t)(tw * th * 4));
-                                tma_load_2d(tile, &tmap, nx, ny, bar);
-                            }
-                            const bool done = __all_sync(kFull, mbar_wait_bounded(bar, phase, 1 << 22));
-                            phase ^= 1u;
-                            if (done) {
-                                tx0 = nx;
-                                ty0 = ny;
-                                tile_ok = true;
-                            } else {
-                                // a copy that never completed: stop staging for this warp
-                                tile_ok = false;
-                                tile_on = false;
-                                if (lane == 0 && a.err) atomicExch(a.err, 1);
-                            }
-                        }
-                    }
-                }
-            }
-            // pass 1: sample, four pixels' loads before their stores
-            float part = 0.0f;
-            int cnt = 0;
-            uint64_t valid = 0;
-            {
-                int row = row0, col = col0;
-                for (int k0 = 0; k0 < K; k0 += 4) {
-                    float v[4];
-                    int ii[4];
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int k = k0 + u;
-                        ii[u] = lane + 32 * k;
-                        v[u] = 0.0f;
-                        if (k < K && ii[u] < n) {
-                            bool inside;
-                            v[u] = fast_sample<SIX>(tile, defI, tw, th, pitch, tx0, ty0, tile_ok, cx, cy, lo_x, hi_x,
-                                                    lo_y, hi_y, W, (float)(col - half), (float)(row - half), inside);
-                            if (inside && ((refok >> k) & 1ull)) {
-                                valid |= 1ull << k;
-                                part = part + v[u];
-                                ++cnt;
-                            }
-                        }
-                        col += r;
-                        row += q;
-                        if (col >= dim) {
-                            col -= dim;
-                            ++row;
-                        }
-                    }
-#pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
-                }
-            }
-            __syncwarp();
-            const float sum = wsum(part);
-            cnt = wsum(cnt);
-            if (cnt < a.min_valid) {
-                res = res_from(W, 1, 2.0f, iter);
-                break;
-            }
-            if (cnt != n) {  // a masked iteration: the general pass solves this task
-                defer = true;
-                break;
             }
             const float mean = sum / (float)cnt;
-            float sq = 0.0f;
-#pragma unroll 4
-            for (int k = 0; k < K; ++k) {
-                if (!((valid >> k) & 1ull)) continue;
-                const float d = vals[lane + 32 * k] - mean;
-                sq = __fmaf_rn(d, d, sq);
-            }
-            float sdev = sqrtf(wsum(sq) / (float)cnt);
+            float sdev = sqrtf(sum_sq(mean, valid) / (float)cnt);
             if (sdev < 1e-5f) sdev = 1.0f;
             const float inv = 1.0f / sdev;
 
-            // pass 3: ZNSSD residual and steepest-descent 6-vector
             float ep = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f, gp3 = 0.0f, gp4 = 0.0f, gp5 = 0.0f;
             {
                 int row = row0, col = col0;
@@ -1062,23 +1088,26 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
                         gp4 = __fmaf_rn(g1 * fx, diff, gp4);
                         gp5 = __fmaf_rn(g1 * fy, diff, gp5);
                     }
-                    col += r;
-                    row += q;
-                    if (col >= dim) {
-                        col -= dim;
-                        ++row;
-                    }
+                    advance(row, col);
                 }
             }
-            const float err = wsum(ep);
+            const float err2 = wsum(ep);
             const float g[6] = {wsum(gp0), wsum(gp1), wsum(gp2), wsum(gp3), wsum(gp4), wsum(gp5)};
-            final_score = err / (float)cnt;
+
+            const double* Hstep = Hr;
+            if constexpr (GENERAL) {
+                if (!full) {
+                    if (!masked_step(valid)) return res_from(Wp, 1, 2.0f, iter);
+                    Hstep = Hm;
+                }
+            }
+            final_score = err2 / (float)cnt;
 
             float dpl = 0.0f;
             if (lane < 6) {
                 double acc = 0.0;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) acc = __fma_rn(Hr[lane * 6 + k], (double)g[k], acc);
+                for (int k = 0; k < 6; ++k) acc = __fma_rn(Hstep[lane * 6 + k], (double)g[k], acc);
                 dpl = (float)(-acc);
             }
             float dp[6];
@@ -1090,30 +1119,24 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
             bool fin = true;
 #pragma unroll
             for (int k = 0; k < 6; ++k) fin = fin && finite_f(dp[k]);
-            if (!fin || !(fabsf(det) > 1e-6f)) {
-                res = res_from(W, 1, 2.0f, iter + 1);
-                break;
-            }
+            if (!fin || !(fabsf(det) > 1e-6f)) return res_from(Wp, 1, 2.0f, iter + 1);
             const float id = 1.0f / det;
             const float i00 = a11 * id, i01 = -a01 * id, i10 = -a10 * id, i11 = a00 * id;
             const float i02 = -(i00 * dp[0] + i01 * dp[1]);
             const float i12 = -(i10 * dp[0] + i11 * dp[1]);
             float Wn[6];
-            Wn[0] = W[0] * i00 + W[1] * i10;
-            Wn[1] = W[0] * i01 + W[1] * i11;
-            Wn[2] = (W[0] * i02 + W[1] * i12) + W[2];
-            Wn[3] = W[3] * i00 + W[4] * i10;
-            Wn[4] = W[3] * i01 + W[4] * i11;
-            Wn[5] = (W[3] * i02 + W[4] * i12) + W[5];
+            Wn[0] = Wp[0] * i00 + Wp[1] * i10;
+            Wn[1] = Wp[0] * i01 + Wp[1] * i11;
+            Wn[2] = (Wp[0] * i02 + Wp[1] * i12) + Wp[2];
+            Wn[3] = Wp[3] * i00 + Wp[4] * i10;
+            Wn[4] = Wp[3] * i01 + Wp[4] * i11;
+            Wn[5] = (Wp[3] * i02 + Wp[4] * i12) + Wp[5];
             bool wfin = true;
 #pragma unroll
             for (int k = 0; k < 6; ++k) wfin = wfin && finite_f(Wn[k]);
-            if (!wfin) {
-                res = res_from(W, 1, 2.0f, iter + 1);
-                break;
-            }
+            if (!wfin) return res_from(Wp, 1, 2.0f, iter + 1);
 #pragma unroll
-            for (int k = 0; k < 6; ++k) W[k] = Wn[k];
+            for (int k = 0; k < 6; ++k) Wp[k] = Wn[k];
 
             float nn = dp[0] * dp[0];
 #pragma unroll
@@ -1132,14 +1155,302 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
                 }
                 const float tx = wsum(sx), ty = wsum(sy);
                 const float sg = ty < tx ? ty : tx;
-                if (sg <= 0.0f || !finite_f(final_score))
-                    res = res_from(W, 1, 2.0f, iter + 1);
-                else
-                    res = res_from(W, 0, final_score, iter + 1);
-                break;
+                if (sg <= 0.0f || !finite_f(final_score)) return res_from(Wp, 1, 2.0f, iter + 1);
+                return res_from(Wp, 0, final_score, iter + 1);
             }
         }
-        // a NO_SEARCH task that would take the Simplex rescue goes to the general pass
+        return res_from(Wp, 1, final_score, kIcgnMaxIter);
+    }
+
+    // evaluate_znssd (optimization_engine.cpp:467-528).
+    __device__ __forceinline__ float znssd(const float Wp[6]) {
+        float sum;
+        uint64_t valid;
+        const int cnt = sample(Wp, sum, valid);
+        if (cnt == 0 || cnt < min_valid) return 2.0f;
+        const float mean = sum / (float)cnt;
+        float sdev = sqrtf(sum_sq(mean, valid) / (float)cnt);
+        if (sdev < 1e-5f) sdev = 1.0f;
+        const bool full = cnt == n;
+        const float inv = 1.0f / sdev;
+        float ep = 0.0f;
+#pragma unroll 4
+        for (int k = 0; k < K; ++k) {
+            if ((valid >> k) & 1ull) {
+                const int i = lane + 32 * k;
+                const float rn = srn[i];
+                const float diff = full ? rn - (vals[i] - mean) * inv : rn - (vals[i] - mean) / sdev;
+                ep = __fmaf_rn(diff, diff, ep);
+            }
+        }
+        const float score = wsum(ep) / (float)cnt;
+        return finite_f(score) ? score : 2.0f;
+    }
+
+    // solve_simplex (optimization_engine.cpp:531-651). Every lane keeps the
+    // same simplex; the evaluations are warp-collective.
+    __device__ __forceinline__ Res simplex(float s0, float s1, float s2, float s3, float s4, float s5, bool trans) {
+        const int D = trans ? 2 : 6, np = D + 1;
+        float p[7][6];
+        float y[7];
+        for (int i = 0; i < 7; ++i) {
+            y[i] = 0.0f;
+            for (int j = 0; j < 6; ++j) p[i][j] = 0.0f;
+        }
+        const float scale[6] = {2.0f, 2.0f, 0.01f, 0.01f, 0.01f, 0.01f};
+        auto eval = [&](const float* pt) {
+            float Wq[6];
+            if (trans) {
+                Wq[0] = 1.0f; Wq[1] = 0.0f; Wq[2] = pt[0]; Wq[3] = 0.0f; Wq[4] = 1.0f; Wq[5] = pt[1];
+            } else {
+                Wq[0] = 1.0f + pt[2]; Wq[1] = pt[3]; Wq[2] = pt[0]; Wq[3] = pt[4]; Wq[4] = 1.0f + pt[5]; Wq[5] = pt[1];
+            }
+            return znssd(Wq);
+        };
+        p[0][0] = s0;
+        p[0][1] = s1;
+        if (!trans) {
+            p[0][2] = s2;
+            p[0][3] = s3;
+            p[0][4] = s4;
+            p[0][5] = s5;
+        }
+        y[0] = eval(p[0]);
+        for (int i = 1; i < np; ++i) {
+            for (int j = 0; j < D; ++j) p[i][j] = p[0][j];
+            p[i][i - 1] += scale[i - 1];
+            y[i] = eval(p[i]);
+        }
+        for (int it = 0; it < 100; ++it) {
+            int idx[7] = {0, 1, 2, 3, 4, 5, 6};
+            for (int aa = 1; aa < np; ++aa) {
+                const int v = idx[aa];
+                int b = aa;
+                while (b > 0 && y[v] < y[idx[b - 1]]) {
+                    idx[b] = idx[b - 1];
+                    --b;
+                }
+                idx[b] = v;
+            }
+            if (fabsf(y[idx[0]] - y[idx[np - 1]]) < 1e-5f) break;
+            float pb[6] = {0, 0, 0, 0, 0, 0};
+            for (int i = 0; i < D; ++i)
+                for (int j = 0; j < D; ++j) pb[j] += p[idx[i]][j];
+            for (int j = 0; j < D; ++j) pb[j] /= (float)D;
+            float pr[6] = {0, 0, 0, 0, 0, 0};
+            for (int j = 0; j < D; ++j) pr[j] = pb[j] + 1.0f * (pb[j] - p[idx[np - 1]][j]);
+            const float yr = eval(pr);
+            if (y[idx[0]] <= yr && yr < y[idx[np - 2]]) {
+                for (int j = 0; j < D; ++j) p[idx[np - 1]][j] = pr[j];
+                y[idx[np - 1]] = yr;
+            } else if (yr < y[idx[0]]) {
+                float pe[6] = {0, 0, 0, 0, 0, 0};
+                for (int j = 0; j < D; ++j) pe[j] = pb[j] + 2.0f * (pr[j] - pb[j]);
+                const float ye = eval(pe);
+                if (ye < yr) {
+                    for (int j = 0; j < D; ++j) p[idx[np - 1]][j] = pe[j];
+                    y[idx[np - 1]] = ye;
+                } else {
+                    for (int j = 0; j < D; ++j) p[idx[np - 1]][j] = pr[j];
+                    y[idx[np - 1]] = yr;
+                }
+            } else {
+                float pc[6] = {0, 0, 0, 0, 0, 0};
+                const bool outside = yr < y[idx[np - 1]];
+                for (int j = 0; j < D; ++j) {
+                    const float bj = outside ? pr[j] : p[idx[np - 1]][j];
+                    pc[j] = pb[j] + 0.5f * (bj - pb[j]);
+                }
+                const float yc = eval(pc);
+                const float ylast = y[idx[np - 1]];
+                if (yc < (ylast < yr ? ylast : yr)) {
+                    for (int j = 0; j < D; ++j) p[idx[np - 1]][j] = pc[j];
+                    y[idx[np - 1]] = yc;
+                } else {
+                    for (int i = 1; i < np; ++i) {
+                        for (int j = 0; j < D; ++j) p[idx[i]][j] = p[idx[0]][j] + 0.5f * (p[idx[i]][j] - p[idx[0]][j]);
+                        y[idx[i]] = eval(p[idx[i]]);
+                    }
+                }
+            }
+        }
+        int best = 0;
+        for (int k = 1; k < np; ++k)
+            if (y[k] < y[best]) best = k;
+        Res res;
+        res.u = p[best][0];
+        res.v = p[best][1];
+        res.ux = trans ? 0.0f : p[best][2];
+        res.uy = trans ? 0.0f : p[best][3];
+        res.vx = trans ? 0.0f : p[best][4];
+        res.vy = trans ? 0.0f : p[best][5];
+        res.status = y[best] > kSimplexFailScore ? -2 : 0;
+        res.score = y[best];
+        res.iters = 0;
+        return res;
+    }
+
+    // estimate_initial_guess (optimization_engine.cpp:120-179): one offset
+    // per lane at a time (8 each), sequential sums as the reference, then the
+    // first minimum in the reference's v-major order. Returns (u, v); the
+    // guess when no offset qualifies.
+    __device__ __forceinline__ float2 coarse(float gu, float gv) const {
+        int sampled = 0;
+        for (int i = 0; i < n; i += 9) ++sampled;
+        float best = 1e20f;
+        int best_idx = 1 << 30;
+        for (int j = 0; j < 8; ++j) {
+            const int idx = lane * 8 + j;  // increasing per lane: first minimum kept
+            const int v = -15 + 2 * (idx / 16), u = -15 + 2 * (idx % 16);
+            auto sample_at = [&](int i, float& rr, float& dd) {
+                const int row = i / dim, col = i - (i / dim) * dim;
+                const float rv = __ldg(refI + ref_base + row * pitch + col);
+                if (rv < kGhost) return false;
+                const int x = cx + (col - half) + u, y = cy + (row - half) + v;
+                if (x < 4 || x > W - 5 || y < 4 || y > H - 5) return false;
+                rr = rv;
+                dd = __ldg(defI + (size_t)y * pitch + x);
+                return true;
+            };
+            int m = 0;
+            float mr = 0.0f, md = 0.0f;
+            for (int i = 0; i < n; i += 9) {
+                float rr, dd;
+                if (!sample_at(i, rr, dd)) continue;
+                mr = mr + rr;
+                md = md + dd;
+                ++m;
+            }
+            if (m < 3 || 2 * m < sampled) continue;
+            const float fm = (float)m;
+            mr = mr / fm;
+            md = md / fm;
+            float vr = 0.0f, vd = 0.0f;
+            for (int i = 0; i < n; i += 9) {
+                float rr, dd;
+                if (!sample_at(i, rr, dd)) continue;
+                vr = vr + (rr - mr) * (rr - mr);
+                vd = vd + (dd - md) * (dd - md);
+            }
+            const float sr = sqrtf(vr / fm), sd = sqrtf(vd / fm);
+            if (!(sr > 1e-5f) || !(sd > 1e-5f)) continue;
+            float score = 0.0f;
+            for (int i = 0; i < n; i += 9) {
+                float rr, dd;
+                if (!sample_at(i, rr, dd)) continue;
+                const float e = (rr - mr) / sr - (dd - md) / sd;
+                score = score + e * e;
+            }
+            score = score / fm;
+            if (score < best) {
+                best = score;
+                best_idx = idx;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float os = __shfl_xor_sync(kFull, best, o);
+            const int oi = __shfl_xor_sync(kFull, best_idx, o);
+            if (os < best || (os == best && oi < best_idx)) {
+                best = os;
+                best_idx = oi;
+            }
+        }
+        if (best_idx < 256 && best < 1e20f)
+            return make_float2((float)(-15 + 2 * (best_idx % 16)), (float)(-15 + 2 * (best_idx / 16)));
+        return make_float2(gu, gv);
+    }
+};
+
+// Set a warp's solver up for a launch: shared-memory arrays, launch
+// constants (copied out of the by-value argument block), tile state, barrier.
+template <bool SIX>
+__device__ __forceinline__ void solver_setup(WarpSolver<SIX>& s, unsigned char* smem, const StagedLayout& L,
+                                             const CUtensorMap* tmap, const float* refI, const float* refGx,
+                                             const float* refGy, const float* defI, int* err, int n, int dim,
+                                             int pitch, int tw, int th, int W, int H, int min_valid, int lm) {
+    const int lane = threadIdx.x & 31;
+    s.bar = reinterpret_cast<uint64_t*>(smem);
+    s.Hr = reinterpret_cast<double*>(smem + 64);
+    s.Hm = reinterpret_cast<double*>(smem + 352);
+    s.tile = reinterpret_cast<float*>(smem + L.off_tile);
+    s.vals = reinterpret_cast<float*>(smem + L.off_vals);
+    s.srn = reinterpret_cast<float*>(smem + L.off_rn);
+    s.sgx = reinterpret_cast<float*>(smem + L.off_gx);
+    s.sgy = reinterpret_cast<float*>(smem + L.off_gy);
+    s.tmap = tmap;
+    s.refI = refI;
+    s.refGx = refGx;
+    s.refGy = refGy;
+    s.defI = defI;
+    s.err = err;
+    s.n = n;
+    s.dim = dim;
+    s.half = dim / 2;
+    s.pitch = pitch;
+    s.tw = tw;
+    s.th = th;
+    s.W = W;
+    s.H = H;
+    s.K = (n + 31) >> 5;
+    s.q = 32 / dim;
+    s.r = 32 - s.q * dim;
+    s.row0 = lane / dim;
+    s.col0 = lane - s.row0 * dim;
+    s.lane = lane;
+    s.min_valid = min_valid;
+    s.lm = lm;
+    s.tx0 = s.ty0 = 0;
+    s.tile_ok = false;
+    s.tile_on = tw > 0;
+    s.phase = 0;
+    if (lane == 0) mbar_init(s.bar, 1);
+    fence_proxy_async_smem();
+    __syncwarp();
+}
+
+// The fast pass over every task: the common case, everything else deferred.
+template <bool SIX>
+__global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
+                                                  const StagedLayout L) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    WarpSolver<SIX> s;
+    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
+                 a.tile_h, a.W, a.H, a.min_valid, a.lm);
+    const int lane = s.lane, dim = s.dim, half = s.half;
+    const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
+    int* const n_deferred = a.queue + 2;
+    int* const deferred = a.deferred;
+    int polled = 0;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(a.queue, 1);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= ntasks) break;
+        // the cancel flag lives in host memory: a read crosses PCIe, so a warp
+        // looks at it once every kCancelPollTasks tasks, not per task
+        if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
+        const dic_task T = a.tasks[t];
+        if (T.mode == DIC_INIT_AUTO_SEARCH || s.K > kFastMaxPerLane) {
+            if (lane == 0) deferred[atomicAdd(n_deferred, 1)] = t;
+            __syncwarp();
+            continue;
+        }
+        dic_result out;
+        out.u = out.v = out.ux = out.uy = out.vx = out.vy = 0.0f;
+        out.score = 0.0f;
+        out.status = out.iters = out.trigger_iters = out.invalid_ref = out.flags = 0;
+        const bool dim_ok = dim >= 3 && (dim & 1) && dim * dim <= a.max_n;
+        const bool on_img = T.cx - half >= 0 && T.cx + half < a.W && T.cy - half >= 0 && T.cy + half < a.H;
+        if (!dim_ok || !on_img || !a.pool_valid[T.node]) {
+            if (lane == 0) a.results[t] = out;
+            continue;
+        }
+        s.begin(T, a.pool_ms[T.node], a.pool_Hs + (size_t)T.node * 21);
+        // calculate_deformation (optimization_engine.cpp:55-118), IC-GN only
+        bool defer = false;
+        Res res = s.template icgn<false>(T.g, defer);
+        // a NO_SEARCH task that would take the Simplex rescue goes to the rescue pass
         if (!defer && T.mode == DIC_INIT_NO_SEARCH && (res.status != 0 || res.score > kCorrSimplexTrigger))
             defer = true;
         if (defer) {
@@ -1147,7 +1458,7 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
             __syncwarp();
             continue;
         }
-        if ((float)ghost / (float)(dim * dim) > kGhostRejectFraction) {
+        if ((float)s.ghost / (float)(dim * dim) > kGhostRejectFraction) {
             res.score = 2.0f;
             res.status = 1;
         }
@@ -1157,7 +1468,7 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
             out.status = res.status;
             out.iters = res.iters;
             out.trigger_iters = res.iters;
-            out.invalid_ref = ghost;
+            out.invalid_ref = s.ghost;
             out.flags = DIC_RES_INITIALIZED;
             a.results[t] = out;
         }
@@ -1165,43 +1476,128 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
     }
 }
 
-constexpr int kFastMaxSmem = 227 * 1024;
-
-// The fast pass (one warp per block, as many blocks as fit on the device at
-// once, persistent) and then the general pass over what it handed on.
+// The rescue pass over the tasks the fast pass handed on, with every path of
+// calculate_deformation (optimization_engine.cpp:55-118): the coarse search
+// and 2-DOF Simplex of AUTO_SEARCH, masked iterations, and the 6-DOF Simplex
+// rescue of NO_SEARCH, keeping the better run.
 template <bool SIX>
-cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const FastLayout& FL, bool fast_ok,
-                          int grid_blocks, size_t smem, cudaStream_t st) {
-    cudaError_t e;
-    if (fast_ok) {
-        e = cudaFuncSetAttribute(fast_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, FL.bytes);
-        if (e != cudaSuccess) return e;
-        int dev = 0, sms = 0, per_sm = 0;
-        e = cudaGetDevice(&dev);
-        if (e != cudaSuccess) return e;
-        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e != cudaSuccess) return e;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fast_kernel<SIX>, 32, FL.bytes);
-        if (e != cudaSuccess) return e;
-        long blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
-        if (blocks > a.n_tasks) blocks = a.n_tasks > 0 ? a.n_tasks : 1;
-        fast_kernel<SIX><<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
+__global__ void __launch_bounds__(32, 1) rescue_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
+                                                       const StagedLayout L) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    WarpSolver<SIX> s;
+    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
+                 a.tile_h, a.W, a.H, a.min_valid, a.lm);
+    const int lane = s.lane, dim = s.dim, half = s.half;
+    const int ntasks = *(volatile const int*)(a.queue + 2);
+    int* const queue = a.queue + 1;
+    int polled = 0;
+    for (;;) {
+        int q = 0;
+        if (lane == 0) q = atomicAdd(queue, 1);
+        q = __shfl_sync(kFull, q, 0);
+        if (q >= ntasks) break;
+        if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
+        const int t = a.deferred[q];
+        const dic_task T = a.tasks[t];
+        dic_result out;
+        out.u = out.v = out.ux = out.uy = out.vx = out.vy = 0.0f;
+        out.score = 0.0f;
+        out.status = out.iters = out.trigger_iters = out.invalid_ref = out.flags = 0;
+        const bool dim_ok = dim >= 3 && (dim & 1) && dim * dim <= a.max_n;
+        const bool on_img = T.cx - half >= 0 && T.cx + half < a.W && T.cy - half >= 0 && T.cy + half < a.H;
+        if (!dim_ok || !on_img || !a.pool_valid[T.node]) {
+            if (lane == 0) a.results[t] = out;
+            continue;
+        }
+        s.begin(T, a.pool_ms[T.node], a.pool_Hs + (size_t)T.node * 21);
+        const int mode = T.mode;
+        float st[6] = {T.g[0], T.g[1], T.g[2], T.g[3], T.g[4], T.g[5]};
+        bool rescue = false;
+        if (mode == DIC_INIT_AUTO_SEARCH) {
+            float2 e = make_float2(st[0], st[1]);
+            if (e.x == 0.0f && e.y == 0.0f) e = s.coarse(e.x, e.y);
+            const Res cr = s.simplex(e.x, e.y, 0.0f, 0.0f, 0.0f, 0.0f, true);
+            rescue = true;
+            st[0] = cr.u; st[1] = cr.v; st[2] = st[3] = st[4] = st[5] = 0.0f;
+        }
+        Res res;
+        int trigger = 0;
+        bool unused = false;
+        for (int run = 0; run < 2; ++run) {
+            const Res r = s.template icgn<true>(st, unused);
+            if (run == 0) {
+                res = r;
+                trigger = r.iters;
+                if (mode != DIC_INIT_NO_SEARCH || !(r.status != 0 || r.score > kCorrSimplexTrigger)) break;
+                const Res rr = s.simplex(T.g[0], T.g[1], T.g[2], T.g[3], T.g[4], T.g[5], false);
+                rescue = true;
+                st[0] = rr.u; st[1] = rr.v; st[2] = rr.ux; st[3] = rr.uy; st[4] = rr.vx; st[5] = rr.vy;
+            } else {
+                const bool first_better = res.status == 0 && (r.status != 0 || res.score < r.score);
+                if (!first_better) res = r;
+            }
+        }
+        if ((float)s.ghost / (float)(dim * dim) > kGhostRejectFraction) {
+            res.score = 2.0f;
+            res.status = 1;
+        }
+        if (lane == 0) {
+            out.u = res.u; out.v = res.v; out.ux = res.ux; out.uy = res.uy; out.vx = res.vx; out.vy = res.vy;
+            out.score = res.score;
+            out.status = res.status;
+            out.iters = res.iters;
+            out.trigger_iters = trigger;
+            out.invalid_ref = s.ghost;
+            out.flags = DIC_RES_INITIALIZED | (rescue ? DIC_RES_RESCUE : 0);
+            a.results[t] = out;
+        }
+        __syncwarp();
     }
-    // the general pass: one warp per block with the whole register file (its
-    // rare paths inline without spilling), as many blocks as fit at once
-    e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
+}
+
+// Blocks of one warp: as many as fit on the device at once (persistent),
+// at most `cap` (when positive) and at most one per task.
+template <class K>
+cudaError_t one_wave(K kernel, size_t smem, long cap, long tasks, long& blocks) {
     int dev = 0, sms = 0, per_sm = 0;
-    e = cudaGetDevice(&dev);
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, solve_kernel<SIX, false>, 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32, smem);
     if (e != cudaSuccess) return e;
-    long blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+    if (cap > 0 && blocks > cap) blocks = cap;
+    if (blocks > tasks) blocks = tasks > 0 ? tasks : 1;
+    return cudaSuccess;
+}
+
+// The fast pass and then the rescue pass over what it handed on; subsets the
+// staged solvers do not take go to solve_kernel, which takes every task.
+template <bool SIX>
+cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const StagedLayout& SL, bool staged_ok,
+                          int grid_blocks, size_t smem, cudaStream_t st) {
     // the caller's hint counts units of kSolveThreads / 32 subsets
-    if (grid_blocks > 0 && blocks > (long)grid_blocks * (kSolveThreads / 32)) blocks = (long)grid_blocks * (kSolveThreads / 32);
-    if (blocks > a.n_tasks) blocks = a.n_tasks > 0 ? a.n_tasks : 1;
+    const long cap = grid_blocks > 0 ? (long)grid_blocks * (kSolveThreads / 32) : 0;
+    long blocks = 1;
+    cudaError_t e;
+    if (staged_ok) {
+        e = cudaFuncSetAttribute(fast_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
+        if (e != cudaSuccess) return e;
+        e = one_wave(fast_kernel<SIX>, SL.bytes, 0, a.n_tasks, blocks);
+        if (e != cudaSuccess) return e;
+        fast_kernel<SIX><<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
+        e = cudaFuncSetAttribute(rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
+        if (e != cudaSuccess) return e;
+        e = one_wave(rescue_kernel<SIX>, SL.bytes, cap, a.n_tasks, blocks);
+        if (e != cudaSuccess) return e;
+        rescue_kernel<SIX><<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
+        return cudaGetLastError();
+    }
+    e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    e = one_wave(solve_kernel<SIX, false>, smem, cap, a.n_tasks, blocks);
+    if (e != cudaSuccess) return e;
     solve_kernel<SIX, false><<<(unsigned)blocks, 32, smem, st>>>(tmap, a);
     return cudaGetLastError();
 }
@@ -1269,11 +1665,11 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     if (e != cudaSuccess) return e;
     // the fast pass takes subsets up to kFastMaxPerLane pixels per lane whose
     // shared memory fits one block; otherwise the general pass takes every task
-    const FastLayout FL = fast_layout(a.n, tw, th);
-    const bool fast_ok = ((a.n + 31) >> 5) <= kFastMaxPerLane && FL.bytes <= kFastMaxSmem;
-    a.general_all = fast_ok ? 0 : 1;
-    return six ? launch_passes<true>(tmap, a, FL, fast_ok, grid_blocks, smem, st)
-               : launch_passes<false>(tmap, a, FL, fast_ok, grid_blocks, smem, st);
+    const StagedLayout SL = staged_layout(a.n, tw, th);
+    const bool staged_ok = ((a.n + 31) >> 5) <= kFastMaxPerLane && SL.bytes <= kFastMaxSmem;
+    a.general_all = staged_ok ? 0 : 1;
+    return six ? launch_passes<true>(tmap, a, SL, staged_ok, grid_blocks, smem, st)
+               : launch_passes<false>(tmap, a, SL, staged_ok, grid_blocks, smem, st);
 }
 
 }  // namespace dic

@@ -121,6 +121,23 @@ def test_solve_bit_exact(six, mode):
     assert (io[:, 1] == 0).sum() > 10
 
 
+@pytest.mark.parametrize("mode", [sb.INIT_NO_SEARCH, sb.INIT_AUTO_SEARCH])
+def test_solve_large_subset_bit_exact(mode):
+    # subset 47 (more than 64 pixels per lane) is solved by the unstaged kernel
+    n = 256
+    ref = sb.speckle(n, n, 4)
+    dfm = sb.speckle(n, n, 4, sb.warp_block(cx=128, cy=128, u0=0.7, v0=-1.4, a=(0.004, 0.0, 0.0, -0.003)), 1.0, 9)
+    rng = np.random.default_rng(8)
+    xy = rng.integers(30, n - 30, size=(24, 2)).astype(np.int32)
+    guess = np.zeros((24, 6), np.float32)
+    if mode == sb.INIT_NO_SEARCH:
+        guess[:, 0], guess[:, 1] = 0.5, -1.0
+        guess[::4, 0] = 5.0
+    res, fo, io = _solve_case(ref, dfm, xy, guess, mode, 47)
+    _assert_same(res, fo, io)
+    assert (io[:, 1] == 0).sum() > 5
+
+
 def test_solve_masked_and_edges_bit_exact():
     n = 200
     ref = sb.speckle(n, n, 9)
