@@ -53,6 +53,19 @@ def lib():
         L.oracle_vsg_window_node_count.argtypes = [ctypes.c_int, ctypes.c_int]
         L.oracle_corpus.argtypes = [ctypes.c_int, ctypes.c_int, _i32p, _f32p, ctypes.c_int]
         L.oracle_ff_inputs.argtypes = [ctypes.c_int, _u8p, _u8p]
+        L.oracle_inc_create.restype = ctypes.c_void_p
+        L.oracle_inc_destroy.argtypes = [ctypes.c_void_p]
+        L.oracle_inc_init.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int, ctypes.c_int, _u8p, _i32p, ctypes.c_int]
+        L.oracle_inc_process.argtypes = [ctypes.c_void_p, _u8p, _f32p, ctypes.c_int, _f32p, ctypes.c_int, _i32p]
+        field = [ctypes.c_int] * 5 + [_f32p] * 7 + [_u8p]
+        L.oracle_inc_sample.argtypes = field + [ctypes.c_float, ctypes.c_float, _f32p]
+        L.oracle_inc_fit.argtypes = field + [ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
+        L.oracle_inc_anchor_need.argtypes = field + [ctypes.c_float, ctypes.c_float, ctypes.c_int]
+        L.oracle_inc_node_field.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p, _u8p, _u8p]
+        L.oracle_inc_warp_mask.argtypes = [_u8p, ctypes.c_int, ctypes.c_int] + [ctypes.c_int] * 5 + \
+            [_f32p, _f32p, _u8p, ctypes.c_int, _u8p]
+        L.oracle_inc_match.argtypes = [_u8p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
         _lib = L
     return _lib
 
@@ -175,3 +188,104 @@ def ff_inputs(scenario: int):
     dfm = np.zeros((320, 320), np.uint8)
     lib().oracle_ff_inputs(scenario, _p(ref, _u8p), _p(dfm, _u8p))
     return ref, dfm
+
+
+# ------------------------------------------------------------------ incremental
+class IncrementalOracle:
+    """The incremental session over the restatement (oracle/src/incremental.hpp)."""
+
+    def __init__(self):
+        self._h = lib().oracle_inc_create()
+
+    def close(self):
+        if self._h:
+            lib().oracle_inc_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def init(self, ref, params, update_interval: int, mask=None) -> int:
+        g = np.ascontiguousarray(ref, np.uint8)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        p = np.asarray(params, np.int32)
+        return lib().oracle_inc_init(self._h, _p(g, _u8p), g.shape[1], g.shape[0], _p(m, _u8p), _p(p, _i32p),
+                                     update_interval)
+
+    def process(self, frame, capacity: int, metrics_len: int = 24):
+        d = np.ascontiguousarray(frame, np.uint8)
+        out = np.zeros(max(capacity, 1), np.float32)
+        met = np.zeros(max(metrics_len, 1), np.float32)
+        info = np.zeros(6, np.int32)
+        rc = lib().oracle_inc_process(self._h, _p(d, _u8p), _p(out, _f32p), capacity, _p(met, _f32p), metrics_len,
+                                      _p(info, _i32p))
+        return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info
+
+
+class NodeField:
+    """A lattice for the incremental math entries: (gw, gh, rx, ry, step) and per-node arrays."""
+
+    def __init__(self, gw, gh, rx, ry, step):
+        self.geom = (gw, gh, rx, ry, step)
+        n = gw * gh
+        self.u, self.v = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.ux, self.uy = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.vx, self.vy = np.zeros(n, np.float32), np.zeros(n, np.float32)
+        self.corr = np.zeros(n, np.float32)
+        self.valid = np.ones(n, np.uint8)
+
+    def node(self, i, j):
+        gw, gh, rx, ry, step = self.geom
+        return float(rx + i * step), float(ry + j * step)
+
+    def _args(self):
+        return list(self.geom) + [_p(a, _f32p) for a in (self.u, self.v, self.ux, self.uy, self.vx, self.vy,
+                                                          self.corr)] + [_p(self.valid, _u8p)]
+
+
+def inc_sample(f: NodeField, x, y):
+    r = np.zeros(4, np.float32)
+    ok = lib().oracle_inc_sample(*f._args(), x, y, _p(r, _f32p))
+    return bool(ok), float(r[0]), float(r[1]), float(r[2]), bool(r[3])
+
+
+def inc_fit(f: NodeField, x, y, radius):
+    r = np.zeros(3, np.float32)
+    ok = lib().oracle_inc_fit(*f._args(), x, y, radius, _p(r, _f32p))
+    return bool(ok), float(r[0]), float(r[1]), float(r[2])
+
+
+def inc_anchor_need(f: NodeField, x, y, subset):
+    return ["drop", "refresh", "keep"][lib().oracle_inc_anchor_need(*f._args(), x, y, subset)]
+
+
+def inc_node_field(u, v, corr, solved):
+    gh, gw = u.shape
+    out = np.zeros(gw * gh, np.uint8)
+    arrs = [np.ascontiguousarray(a, np.float32).ravel() for a in (u, v, corr)]
+    s = np.ascontiguousarray(solved, np.uint8).ravel()
+    rej = lib().oracle_inc_node_field(gw, gh, _p(arrs[0], _f32p), _p(arrs[1], _f32p), _p(arrs[2], _f32p),
+                                      _p(s, _u8p), _p(out, _u8p))
+    return out.reshape(gh, gw), rej
+
+
+def inc_warp_mask(mask0, geom, U, V, valid, margin):
+    m = np.ascontiguousarray(mask0, np.uint8)
+    H, W = m.shape
+    out = np.zeros_like(m)
+    U = np.ascontiguousarray(U, np.float32).ravel()
+    V = np.ascontiguousarray(V, np.float32).ravel()
+    valid = np.ascontiguousarray(valid, np.uint8).ravel()
+    lib().oracle_inc_warp_mask(_p(m, _u8p), W, H, *geom, _p(U, _f32p), _p(V, _f32p), _p(valid, _u8p), margin,
+                               _p(out, _u8p))
+    return out
+
+
+def inc_match(ref, dfm, x, y, subset, gx, gy, max_shift):
+    """make_anchor on ref at (x, y) and match_anchor on dfm. Returns (rc, x, y, corr, ax, ay, dx, dy); rc -1
+    when no anchor is cut."""
+    r = np.ascontiguousarray(ref, np.uint8)
+    d = np.ascontiguousarray(dfm, np.uint8)
+    out = np.full(7, -1.0, np.float32)
+    rc = lib().oracle_inc_match(_p(r, _u8p), _p(d, _u8p), r.shape[1], r.shape[0], x, y, subset, gx, gy, max_shift,
+                                _p(out, _f32p))
+    return (rc,) + tuple(float(v) for v in out)

@@ -8,6 +8,7 @@
 #include <memory>
 #include <vector>
 
+#include "incremental.hpp"
 #include "pipeline.hpp"
 #include "refsynth.hpp"
 
@@ -234,6 +235,112 @@ void oracle_ff_inputs(int scenario, uint8_t* ref, uint8_t* def) {
     const std::vector<uint8_t> dd = gray8(def_image(field, W, H, d));
     std::memcpy(ref, r.data(), r.size());
     std::memcpy(def, dd.data(), dd.size());
+}
+
+// ---- incremental session and its per-node math (incremental_core.hpp) ----
+
+void* oracle_inc_create() { return new IncSession(); }
+void oracle_inc_destroy(void* p) { delete static_cast<IncSession*>(p); }
+
+int oracle_inc_init(void* p, const uint8_t* ref, int w, int h, const uint8_t* mask, const int32_t prm[8],
+                    int interval) {
+    IncSession* S = static_cast<IncSession*>(p);
+    semper_inc::IncParams q;
+    q.rect_x = prm[0]; q.rect_y = prm[1]; q.rect_w = prm[2]; q.rect_h = prm[3];
+    q.step = prm[4]; q.subset_size = prm[5]; q.strain_window = prm[6]; q.six = prm[7] != 0;
+    return S->core.init(ref, w, h, mask, q, interval);
+}
+
+// info: reference_frame, reference_updated, tracked_points, frame0_points, taylor_fallbacks, lost_this_frame
+int oracle_inc_process(void* p, const uint8_t* def, float* out, int capacity, float* metrics, int metrics_len,
+                       int32_t info[6]) {
+    IncSession* S = static_cast<IncSession*>(p);
+    semper_inc::FrameInfo fi;
+    const int rc = S->core.process(def, out, capacity, metrics, metrics_len, nullptr, &fi);
+    if (info) {
+        info[0] = fi.reference_frame; info[1] = fi.reference_updated ? 1 : 0; info[2] = fi.tracked_points;
+        info[3] = fi.frame0_points; info[4] = fi.taylor_fallbacks; info[5] = fi.lost_this_frame;
+    }
+    return rc;
+}
+
+static semper_inc::NodeField make_field(int gw, int gh, int rx, int ry, int step, const float* u, const float* v,
+                                        const float* ux, const float* uy, const float* vx, const float* vy,
+                                        const float* corr, const uint8_t* valid) {
+    semper_inc::NodeField f;
+    f.gridW = gw; f.gridH = gh; f.rect_x = rx; f.rect_y = ry; f.step = step;
+    const size_t n = (size_t)gw * gh;
+    f.u.assign(u, u + n); f.v.assign(v, v + n); f.ux.assign(ux, ux + n); f.uy.assign(uy, uy + n);
+    f.vx.assign(vx, vx + n); f.vy.assign(vy, vy + n); f.corr.assign(corr, corr + n); f.valid.assign(valid, valid + n);
+    return f;
+}
+
+// res: u, v, corr, taylor; returns ok
+int oracle_inc_sample(int gw, int gh, int rx, int ry, int step, const float* u, const float* v, const float* ux,
+                      const float* uy, const float* vx, const float* vy, const float* corr, const uint8_t* valid,
+                      float x, float y, float* res) {
+    const semper_inc::IncrementSample s =
+        semper_inc::sample_increment(make_field(gw, gh, rx, ry, step, u, v, ux, uy, vx, vy, corr, valid), x, y);
+    res[0] = s.u; res[1] = s.v; res[2] = s.corr; res[3] = s.taylor ? 1.f : 0.f;
+    return s.ok ? 1 : 0;
+}
+
+int oracle_inc_fit(int gw, int gh, int rx, int ry, int step, const float* u, const float* v, const float* ux,
+                   const float* uy, const float* vx, const float* vy, const float* corr, const uint8_t* valid,
+                   float x, float y, float radius, float* res) {
+    const semper_inc::IncrementSample s = semper_inc::fit_increment(
+        make_field(gw, gh, rx, ry, step, u, v, ux, uy, vx, vy, corr, valid), x, y, radius);
+    res[0] = s.u; res[1] = s.v; res[2] = s.corr;
+    return s.ok ? 1 : 0;
+}
+
+// 0 drop, 1 refresh, 2 keep
+int oracle_inc_anchor_need(int gw, int gh, int rx, int ry, int step, const float* u, const float* v,
+                           const float* ux, const float* uy, const float* vx, const float* vy, const float* corr,
+                           const uint8_t* valid, float x, float y, int subset) {
+    const semper_inc::NodeField f = make_field(gw, gh, rx, ry, step, u, v, ux, uy, vx, vy, corr, valid);
+    const semper_inc::AnchorNeed n = semper_inc::anchor_need(f, semper_inc::gap_distance(f), x, y, subset);
+    return n == semper_inc::AnchorNeed::kDrop ? 0 : n == semper_inc::AnchorNeed::kRefresh ? 1 : 2;
+}
+
+// the node field's valid flags after node_field_from_capture; returns the count rejected
+int oracle_inc_node_field(int gw, int gh, const float* u, const float* v, const float* corr, const uint8_t* solved,
+                          uint8_t* valid_out) {
+    semper_inc::SolveCapture c;
+    c.gridW = gw; c.gridH = gh; c.step = 10;
+    const size_t n = (size_t)gw * gh;
+    c.u.assign(u, u + n); c.v.assign(v, v + n);
+    c.ux.assign(n, 0.f); c.uy.assign(n, 0.f); c.vx.assign(n, 0.f); c.vy.assign(n, 0.f);
+    c.corr.assign(corr, corr + n); c.solved.assign(solved, solved + n);
+    int rejected = 0;
+    const semper_inc::NodeField f = semper_inc::node_field_from_capture(c, &rejected);
+    std::memcpy(valid_out, f.valid.data(), n);
+    return rejected;
+}
+
+void oracle_inc_warp_mask(const uint8_t* mask0, int W, int H, int gw, int gh, int rx, int ry, int step,
+                          const float* U, const float* V, const uint8_t* valid, int margin, uint8_t* out) {
+    const size_t n = (size_t)gw * gh;
+    const std::vector<uint8_t> m(mask0, mask0 + (size_t)W * H);
+    const std::vector<uint8_t> w = semper_inc::warp_material_mask(
+        m, W, H, semper_inc::GridGeom{gw, gh, rx, ry, step}, std::vector<float>(U, U + n),
+        std::vector<float>(V, V + n), std::vector<unsigned char>(valid, valid + n), margin);
+    std::memcpy(out, w.data(), w.size());
+}
+
+// make_anchor on `ref` at (x, y), then match_anchor on `def`; xyc: x, y, corr,
+// and the anchor's ax, ay, dx, dy. Returns -1 when no anchor is cut, else 0/1.
+int oracle_inc_match(const uint8_t* ref, const uint8_t* def, int W, int H, float x, float y, int subset, float gx,
+                     float gy, float max_shift, float* xyc) {
+    semper_inc::CoastAnchor a;
+    if (!semper_inc::make_anchor(ref, W, H, x, y, subset, a)) return -1;
+    Image<float> D;
+    D.prepare(W, H, def);
+    xyc[3] = (float)a.ax; xyc[4] = (float)a.ay; xyc[5] = a.dx; xyc[6] = a.dy;
+    float mx = 0, my = 0, corr = 0;
+    const bool ok = IncBackend::match_on(a, D, subset, false, gx, gy, max_shift, mx, my, corr);
+    if (ok) { xyc[0] = mx; xyc[1] = my; xyc[2] = corr; }
+    return ok ? 1 : 0;
 }
 
 }  // extern "C"

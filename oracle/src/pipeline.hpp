@@ -208,6 +208,43 @@ struct SolveInfo {
     int accepted = 0, attempted = 0, solved = 0;
 };
 
+struct PackOut {
+    int valid_count = 0, dropped_outlier = 0, dropped_post = 0;
+};
+
+// pack_full_field_output (full_field_solver_stats.cpp:21-91) over a grid:
+// the displacement median test, VSG strain, then the row-major packing of
+// the first points that fit, strain failures dropped.
+inline PackOut pack_field(const std::vector<GridPoint>& grid, int gridW, int gridH, int step, int window, float* out,
+                          int capacity) {
+    PackOut po;
+    const size_t NG = (size_t)gridW * gridH;
+    DispField df;
+    df.width = gridW; df.height = gridH; df.step = step;
+    df.u.assign(NG, 0.f); df.v.assign(NG, 0.f); df.valid.assign(NG, 0);
+    for (size_t i = 0; i < NG; ++i)
+        if (grid[i].solved && grid[i].corr >= 0.f) {
+            df.u[i] = grid[i].u;
+            df.v[i] = grid[i].v;
+            df.valid[i] = 1;
+        }
+    po.dropped_outlier = reject_outliers(df);
+    const StrainOut so = vsg_strain(df, window);
+    bool trunc = false;
+    for (int y = 0; y < gridH && !trunc; ++y)
+        for (int x = 0; x < gridW; ++x) {
+            const size_t idx = (size_t)y * gridW + x;
+            if (!df.valid[idx]) continue;
+            if ((po.valid_count + 1) * 8 > capacity) { trunc = true; break; }
+            if (so.exx[idx] <= kStrainFailSentinel) { po.dropped_post++; continue; }
+            float* o = out + (size_t)po.valid_count * 8;
+            o[0] = grid[idx].x; o[1] = grid[idx].y; o[2] = df.u[idx]; o[3] = df.v[idx];
+            o[4] = so.exx[idx]; o[5] = so.eyy[idx]; o[6] = so.exy[idx]; o[7] = grid[idx].corr;
+            po.valid_count++;
+        }
+    return po;
+}
+
 template <class T>
 int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* mask, Params params,
                    float* out, int capacity, float* metrics, int metrics_len, const double* model_H,
@@ -843,30 +880,8 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
 
     // ---------------------------------------------------- pack + strain --
     const auto t_strain = clk::now();
-    DispField df;
-    df.width = gridW; df.height = gridH; df.step = params.step;
-    df.u.assign(NG, 0.f); df.v.assign(NG, 0.f); df.valid.assign(NG, 0);
-    for (size_t i = 0; i < NG; ++i)
-        if (grid[i].solved && grid[i].corr >= 0.f) {
-            df.u[i] = grid[i].u;
-            df.v[i] = grid[i].v;
-            df.valid[i] = 1;
-        }
-    const int dropped_outlier = reject_outliers(df);
-    const StrainOut so = vsg_strain(df, params.strain_window);
-    int valid_count = 0, dropped_post = 0;
-    bool trunc = false;
-    for (int y = 0; y < gridH && !trunc; ++y)
-        for (int x = 0; x < gridW; ++x) {
-            const size_t idx = (size_t)y * gridW + x;
-            if (!df.valid[idx]) continue;
-            if ((valid_count + 1) * 8 > capacity) { trunc = true; break; }
-            if (so.exx[idx] <= kStrainFailSentinel) { dropped_post++; continue; }
-            float* o = out + (size_t)valid_count * 8;
-            o[0] = grid[idx].x; o[1] = grid[idx].y; o[2] = df.u[idx]; o[3] = df.v[idx];
-            o[4] = so.exx[idx]; o[5] = so.eyy[idx]; o[6] = so.exy[idx]; o[7] = grid[idx].corr;
-            valid_count++;
-        }
+    const PackOut po = pack_field(grid, gridW, gridH, params.step, params.strain_window, out, capacity);
+    const int valid_count = po.valid_count, dropped_outlier = po.dropped_outlier, dropped_post = po.dropped_post;
     const double ms_strain = ms_since(t_strain);
     const double ms_total = ms_since(t_total);
 

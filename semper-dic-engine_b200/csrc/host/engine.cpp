@@ -386,6 +386,52 @@ struct Engine::Impl {
 
     int pitch() const { return (E.W_ + 3) & ~3; }
 
+    // pack_full_field_output (full_field_solver_stats.cpp:21-91) over the
+    // field buffers: the displacement median test, VSG strain and packing on
+    // the device, into d_out_p (capacity floats). Returns the points written;
+    // records ev[8] after the packing.
+    int strain_pack(int gW, int gH, int rect_x, int rect_y, int step, int window, float* d_out_p, int capacity,
+                    int& dropped_outlier, int& dropped_post) {
+        cudaStream_t st = E.stream_;
+        const size_t NG = (size_t)gW * gH;
+        valid.ensure(NG); fail.ensure(NG); exx.ensure(NG); eyy.ensure(NG); exy.ensure(NG);
+        launched(1, dic::launch_valid((int)NG, field(), valid.p, st), "valid");
+        dropped_outlier = 0;
+        for (int pass = 0; pass < 5; ++pass) {
+            check(cudaMemsetAsync(counters.p + 3, 0, sizeof(int), st), "memset");
+            launched(1, dic::launch_median_pass(gW, gH, fu.p, fv.p, valid.p, fail.p, counters.p + 3, st), "median");
+            int nf = 0;
+            check(cudaMemcpyAsync(&nf, counters.p + 3, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H fail");
+            sync();
+            if (nf == 0) break;
+            launched(1, dic::launch_clear_failed((int)NG, valid.p, fail.p, st), "clear");
+            dropped_outlier += nf;
+        }
+        launched(1, dic::launch_vsg(gW, gH, step, window, fu.p, fv.p, valid.p, exx.p, eyy.p, exy.p, st), "vsg");
+        const size_t scr = dic::pack_scratch_bytes((int)NG);
+        pack_scratch.ensure(std::max(pack_scratch.n, scr));
+        check(cudaMemsetAsync(counters.p + 4, 0, 3 * sizeof(int), st), "memset");
+        const int max_pts = capacity / 8;
+        launched(4, dic::launch_pack(gW, gH, rect_x, rect_y, step, max_pts, valid.p, fu.p, fv.p, fcorr.p, exx.p, eyy.p,
+                                     exy.p, d_out_p, counters.p + 4, counters.p + 5, pack_scratch.p, pack_scratch.n, st),
+                 "pack");
+        int cnts[3] = {0, 0, 0};
+        check(cudaMemcpyAsync(cnts, counters.p + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H pack");
+        check(cudaEventRecord(ev[8], st), "event");
+        sync();
+        dropped_post = cnts[0];
+        return std::min(cnts[1] + cnts[2], max_pts);
+    }
+
+    // The patch reference of an anchor match: its gray bytes, prepared planes,
+    // pool entry, task and result.
+    DevBuf<uint8_t> aGray, aSkip, aValid;
+    DevBuf<float> aI, aGx, aGy, aMs;
+    DevBuf<double> aHs;
+    DevBuf<dic_task> aTask;
+    DevBuf<dic_result> aRes;
+    DevBuf<int> aQ;
+
     void prepare_deformed(const uint8_t* d_def) {
         const size_t n = (size_t)pitch() * E.H_;
         dI.ensure(n);
@@ -500,6 +546,97 @@ int Engine::run(const uint8_t* def_gray, const uint8_t* mask, Params p, float* o
         check(cudaStreamSynchronize(stream_), "output sync");
     }
     return rc;
+}
+
+int check_params(Params& p, int width, int height) { return validate_params(p, width, height); }
+int vsg_window_nodes(int step, int window) { return vsg_window_node_count(step, window); }
+
+int Engine::pack_field(int gW, int gH, int rect_x, int rect_y, int step, int window, const float* u, const float* v,
+                       const float* corr, const uint8_t* solved, float* out, int capacity) {
+    Impl& I = *impl_;
+    if (gW <= 0 || gH <= 0 || step <= 0 || !u || !v || !corr || !solved || !out) return -3;
+    const size_t NG = (size_t)gW * gH;
+    for (DevBuf<float>* b : {&I.fu, &I.fv, &I.fux, &I.fuy, &I.fvx, &I.fvy, &I.fcorr}) b->ensure(std::max(b->n, NG));
+    I.fsolved.ensure(std::max(I.fsolved.n, NG));
+    I.fiters.ensure(std::max(I.fiters.n, NG));
+    check(cudaMemcpyAsync(I.fu.p, u, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D u");
+    check(cudaMemcpyAsync(I.fv.p, v, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D v");
+    check(cudaMemcpyAsync(I.fcorr.p, corr, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D corr");
+    check(cudaMemcpyAsync(I.fsolved.p, solved, NG, cudaMemcpyHostToDevice, stream_), "H2D solved");
+    const int cap = std::max(capacity, 0);
+    I.d_out.ensure(std::max<size_t>(I.d_out.n, (size_t)std::max(cap, 8)));
+    int dropped_outlier = 0, dropped_post = 0;
+    const int n = I.strain_pack(gW, gH, rect_x, rect_y, step, window, I.d_out.p, cap, dropped_outlier, dropped_post);
+    if (n > 0) {
+        check(cudaMemcpyAsync(out, I.d_out.p, (size_t)n * 8 * sizeof(float), cudaMemcpyDeviceToHost, stream_),
+              "D2H packed");
+        check(cudaStreamSynchronize(stream_), "sync");
+    }
+    return n;
+}
+
+PatchSolve Engine::solve_patch(const uint8_t* patch, int size, int ax, int ay, float gu, float gv, int subset,
+                               bool six) {
+    Impl& I = *impl_;
+    PatchSolve r;
+    if (!has_ref_ || !I.dI.p || !patch || size < subset || subset < 3 || (subset & 1) == 0) return r;
+    cudaStream_t st = stream_;
+    const int pp = (size + 3) & ~3, c = size / 2;
+    const size_t n = (size_t)size * size, planes = (size_t)pp * size;
+    I.aGray.ensure(std::max(I.aGray.n, n));
+    for (DevBuf<float>* b : {&I.aI, &I.aGx, &I.aGy}) b->ensure(std::max(b->n, planes));
+    I.aSkip.ensure(1);
+    I.aValid.ensure(1);
+    I.aMs.ensure(2);
+    I.aHs.ensure(21);
+    I.aTask.ensure(1);
+    I.aRes.ensure(1);
+    I.aQ.ensure(16);
+    check(cudaMemcpyAsync(I.aGray.p, patch, n, cudaMemcpyHostToDevice, st), "H2D patch");
+    I.launched(1, dic::launch_image_prep(I.aGray.p, nullptr, size, size, pp, I.aI.p, I.aGx.p, I.aGy.p, st),
+               "patch prep");
+    check(cudaMemsetAsync(I.aSkip.p, 0, 1, st), "memset");
+    I.launched(1, dic::launch_pool(I.aI.p, I.aGx.p, I.aGy.p, size, size, pp, I.aSkip.p, 1, 1, c, c, 1, subset, 1,
+                                   I.aValid.p, reinterpret_cast<float2*>(I.aMs.p), nullptr, I.aHs.p, st),
+               "patch pool");
+    dic_task t{};
+    t.node = 0;
+    t.cx = ax;
+    t.cy = ay;
+    t.mode = DIC_INIT_NO_SEARCH;
+    t.g[0] = gu;
+    t.g[1] = gv;
+    check(cudaMemcpyAsync(I.aTask.p, &t, sizeof(t), cudaMemcpyHostToDevice, st), "H2D patch task");
+    dic::SolveArgs a = I.solve_args(subset, six ? 1 : 0);
+    a.refI = I.aI.p;
+    a.refGx = I.aGx.p;
+    a.refGy = I.aGy.p;
+    a.ref_pitch = pp;
+    a.ref_dx = c - ax;
+    a.ref_dy = c - ay;
+    a.pool_valid = I.aValid.p;
+    a.pool_ms = reinterpret_cast<const float2*>(I.aMs.p);
+    a.pool_Hs = I.aHs.p;
+    a.tasks = I.aTask.p;
+    a.n_tasks = 1;
+    a.n_tasks_dev = nullptr;
+    a.results = I.aRes.p;
+    a.queue = I.aQ.p;
+    a.deferred = I.aQ.p + 8;
+    I.launched(2, dic::launch_solve(a, six ? 1 : 0, 1, st), "patch solve");
+    dic_result res{};
+    check(cudaMemcpyAsync(&res, I.aRes.p, sizeof(res), cudaMemcpyDeviceToHost, st), "D2H patch result");
+    check(cudaStreamSynchronize(st), "sync");
+    r.initialized = (res.flags & DIC_RES_INITIALIZED) != 0;
+    r.status = res.status;
+    r.score = res.score;
+    r.u = res.u;
+    r.v = res.v;
+    r.ux = res.ux;
+    r.uy = res.uy;
+    r.vx = res.vx;
+    r.vy = res.vy;
+    return r;
 }
 
 int Engine::run_device(const uint8_t* d_def, const uint8_t* mask, Params p, float* d_out, int capacity,
@@ -1161,36 +1298,9 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
 
         // ---------------------------------------------------------------- pack + strain
         const auto t_strain = clk::now();
-        valid.ensure(NG); fail.ensure(NG); exx.ensure(NG); eyy.ensure(NG); exy.ensure(NG);
-        launched(1, dic::launch_valid((int)NG, field(), valid.p, st), "valid");
-        int dropped_outlier = 0;
-        for (int pass = 0; pass < 5; ++pass) {
-            check(cudaMemsetAsync(counters.p + 3, 0, sizeof(int), st), "memset");
-            launched(1, dic::launch_median_pass(gW, gH, fu.p, fv.p, valid.p, fail.p, counters.p + 3, st), "median");
-            int nf = 0;
-            check(cudaMemcpyAsync(&nf, counters.p + 3, sizeof(int), cudaMemcpyDeviceToHost, st), "D2H fail");
-            sync();
-            if (nf == 0) break;
-            launched(1, dic::launch_clear_failed((int)NG, valid.p, fail.p, st), "clear");
-            dropped_outlier += nf;
-        }
-        launched(1, dic::launch_vsg(gW, gH, params.step, params.strain_window, fu.p, fv.p, valid.p, exx.p, eyy.p, exy.p, st),
-              "vsg");
-        const size_t scr = dic::pack_scratch_bytes((int)NG);
-        pack_scratch.ensure(std::max(pack_scratch.n, scr));
-        check(cudaMemsetAsync(counters.p + 4, 0, 3 * sizeof(int), st), "memset");
-        const int max_pts = capacity / 8;
-        launched(4, dic::launch_pack(gW, gH, params.rect_x, params.rect_y, params.step, max_pts, valid.p, fu.p, fv.p,
-                               fcorr.p, exx.p, eyy.p, exy.p, d_out_p, counters.p + 4, counters.p + 5, pack_scratch.p,
-                               pack_scratch.n, st),
-              "pack");
-        int cnts[3] = {0, 0, 0};
-        check(cudaMemcpyAsync(cnts, counters.p + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H pack");
-        check(cudaEventRecord(ev[8], st), "event");
-        sync();
-        const int emits = cnts[1] + cnts[2];
-        const int valid_count = std::min(emits, max_pts);
-        const int dropped_post = cnts[0];
+        int dropped_outlier = 0, dropped_post = 0;
+        const int valid_count = strain_pack(gW, gH, params.rect_x, params.rect_y, params.step, params.strain_window,
+                                            d_out_p, capacity, dropped_outlier, dropped_post);
         const double ms_strain = ms_since(t_strain);
         ticker.stop();
         if (progress) {

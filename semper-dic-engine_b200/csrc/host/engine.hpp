@@ -77,6 +77,19 @@ struct PhaseTimes {
     int launches = 0;                  // kernels this library launched during the solve
 };
 
+// validate_params (full_field_solver.cpp:97-111): clips the rect; 0 or a
+// negative code.
+int check_params(Params& p, int width, int height);
+// StrainCalculator::vsg_window_node_count (strain_calculator.cpp:12-25).
+int vsg_window_nodes(int step, int window);
+
+// The raw result of one patch-subset solve (match_anchor's solve).
+struct PatchSolve {
+    bool initialized = false;
+    int status = 0;
+    float score = 0, u = 0, v = 0, ux = 0, uy = 0, vx = 0, vy = 0;
+};
+
 class Engine {
 public:
     Engine();
@@ -106,6 +119,18 @@ public:
     int run_device(const uint8_t* d_def, const uint8_t* mask, Params p, float* d_out, int capacity,
                    float* metrics, int metrics_len, const double* model_H = nullptr, Progress progress = nullptr,
                    Capture* capture = nullptr);
+
+    // pack_full_field_output over a host grid (gW x gH nodes at rect + i *
+    // step): the displacement median test, VSG strain and packing on the
+    // device, out (host) receiving the points. Returns the points written.
+    int pack_field(int gW, int gH, int rect_x, int rect_y, int step, int window, const float* u, const float* v,
+                   const float* corr, const uint8_t* solved, float* out, int capacity);
+
+    // match_anchor's solve (incremental_math.cpp:238-276): the subset (side
+    // `subset`) at the centre of a size x size gray patch, whose centre pixel
+    // sits at (ax, ay), solved in NO_SEARCH mode on the deformed frame of the
+    // last run from the guess (gu, gv) of its displacement.
+    PatchSolve solve_patch(const uint8_t* patch, int size, int ax, int ay, float gu, float gv, int subset, bool six);
 
     void request_cancel() { h_cancel_[0] = 1; }
     void clear_cancel() { h_cancel_[0] = 0; }

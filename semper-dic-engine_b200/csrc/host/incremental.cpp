@@ -1,65 +1,132 @@
-// IncrementalSession over the device engine: see incremental.hpp.
+// IncrementalSession over the device engine: the session logic of
+// incremental_core.hpp, every solve, adoption and packing on the device.
 #include "incremental.hpp"
 
 #include <cmath>
 #include <cstring>
 
+#include "incremental_core.hpp"
+
 namespace semper_b200 {
+
+namespace {
+
+Params to_params(const semper_inc::IncParams& p) {
+    Params q;
+    q.rect_x = p.rect_x;
+    q.rect_y = p.rect_y;
+    q.rect_w = p.rect_w;
+    q.rect_h = p.rect_h;
+    q.step = p.step;
+    q.subset_size = p.subset_size;
+    q.strain_window = p.strain_window;
+    q.six = p.six;
+    return q;
+}
+
+semper_inc::IncParams from_params(const Params& q) {
+    semper_inc::IncParams p;
+    p.rect_x = q.rect_x;
+    p.rect_y = q.rect_y;
+    p.rect_w = q.rect_w;
+    p.rect_h = q.rect_h;
+    p.step = q.step;
+    p.subset_size = q.subset_size;
+    p.strain_window = q.strain_window;
+    p.six = q.six;
+    return p;
+}
+
+// The solver backend of the session: the device engine.
+struct DeviceBackend {
+    Engine& e;
+
+    int validate(semper_inc::IncParams& p, int W, int H) {
+        Params q = to_params(p);
+        const int rc = check_params(q, W, H);
+        p = from_params(q);
+        return rc;
+    }
+    int vsg_count(int step, int window) { return vsg_window_nodes(step, window); }
+    int set_reference(const uint8_t* gray, int W, int H, const uint8_t* mask) {
+        return e.set_reference(gray, W, H, mask);
+    }
+    int run(const uint8_t* def, const uint8_t* mask, const semper_inc::IncParams& p, float* out, int capacity,
+            float* metrics, int metrics_len, const std::function<void(int)>& progress,
+            semper_inc::SolveCapture* cap) {
+        Capture c;
+        const int rc = e.run(def, mask, to_params(p), out, capacity, metrics, metrics_len, nullptr, progress, &c);
+        if (rc < 0) return rc;
+        cap->gridW = c.gridW;
+        cap->gridH = c.gridH;
+        cap->rect_x = c.rect_x;
+        cap->rect_y = c.rect_y;
+        cap->step = c.step;
+        cap->attempted = c.attempted;
+        cap->u = std::move(c.u);
+        cap->v = std::move(c.v);
+        cap->ux = std::move(c.ux);
+        cap->uy = std::move(c.uy);
+        cap->vx = std::move(c.vx);
+        cap->vy = std::move(c.vy);
+        cap->corr = std::move(c.corr);
+        cap->solved = std::move(c.solved);
+        return rc;
+    }
+    int adopt(const uint8_t* mask) { return e.adopt_last_deformed(mask); }
+    int pack(const semper_inc::GridGeom& g, int window, const std::vector<float>& u, const std::vector<float>& v,
+             const std::vector<float>& corr, const std::vector<unsigned char>& solved, float* out, int capacity) {
+        return e.pack_field(g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, window, u.data(), v.data(), corr.data(),
+                            solved.data(), out, capacity);
+    }
+    bool match_anchor(const semper_inc::CoastAnchor& a, int subset, bool six, float gx, float gy, float max_shift,
+                      float& x, float& y, float& corr) {
+        // guess for the centre pixel: the node's guess less its offset from it
+        const PatchSolve r = e.solve_patch(a.patch.data(), a.size, a.ax, a.ay, gx - a.dx - (float)a.ax,
+                                           gy - a.dy - (float)a.ay, subset, six);
+        if (!r.initialized) return false;
+        return semper_inc::accept_anchor_match(a, r.status, r.score, r.u, r.v, r.ux, r.uy, r.vx, r.vy, gx, gy,
+                                               max_shift, x, y, corr);
+    }
+};
+
+}  // namespace
 
 struct IncrementalSession::Impl {
     Engine engine;
-    bool init = false;
-    Params params;
-    int interval = 0;
-    int W = 0, H = 0;
-    std::vector<uint8_t> mask;
-    int frames = 0;
-    int frame0_points = 0;
+    DeviceBackend backend{engine};
+    semper_inc::IncrementalCore<DeviceBackend> core{backend};
 };
 
 IncrementalSession::IncrementalSession() : impl_(new Impl()) {}
 IncrementalSession::~IncrementalSession() = default;
 
 void IncrementalSession::reset() {
-    impl_->init = false;
-    impl_->frames = 0;
+    impl_->core.clear();
     impl_->engine.reset();
 }
 
-bool IncrementalSession::initialized() const { return impl_->init; }
-int IncrementalSession::frames_processed() const { return impl_->frames; }
+bool IncrementalSession::initialized() const { return impl_->core.initialized(); }
+int IncrementalSession::frames_processed() const { return impl_->core.frames_processed(); }
 Engine& IncrementalSession::engine() { return impl_->engine; }
 
 int IncrementalSession::init(const uint8_t* ref, int w, int h, const uint8_t* mask, const Params& p,
                              int update_interval) {
-    reset();
-    if (!ref || w <= 0 || h <= 0 || update_interval < 0) return -3;
-    Impl& I = *impl_;
-    if (I.engine.set_reference(ref, w, h, mask) != 0) return -3;
-    I.params = p;
-    I.interval = update_interval;
-    I.W = w;
-    I.H = h;
-    I.mask = mask ? std::vector<uint8_t>(mask, mask + (size_t)w * h) : std::vector<uint8_t>();
-    if (update_interval != 0) return -3;  // only the fixed-reference mode in this build so far
-    I.init = true;
-    return 0;
+    impl_->engine.reset();
+    return impl_->core.init(ref, w, h, mask, from_params(p), update_interval);
 }
 
 int IncrementalSession::process(const uint8_t* def, float* out, int capacity, float* metrics, int metrics_len,
                                 Progress progress, FrameInfo* info) {
-    Impl& I = *impl_;
-    if (!I.init) return -3;
-    const int rc = I.engine.run(def, I.mask.empty() ? nullptr : I.mask.data(), I.params, out, capacity, metrics,
-                                metrics_len, nullptr, progress);
-    if (rc >= 0) {
-        I.frames++;
-        if (info) {
-            info->reference_frame = 0;
-            info->reference_updated = false;
-            info->frame0_points = 0;
-            info->tracked_points = 0;
-        }
+    semper_inc::FrameInfo fi;
+    const int rc = impl_->core.process(def, out, capacity, metrics, metrics_len, progress, &fi);
+    if (info) {
+        info->reference_frame = fi.reference_frame;
+        info->reference_updated = fi.reference_updated;
+        info->tracked_points = fi.tracked_points;
+        info->frame0_points = fi.frame0_points;
+        info->taylor_fallbacks = fi.taylor_fallbacks;
+        info->lost_this_frame = fi.lost_this_frame;
     }
     return rc;
 }

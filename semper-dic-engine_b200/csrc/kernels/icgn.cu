@@ -820,6 +820,7 @@ struct WarpSolver {
     const float* defI;
     int* err;
     int n, dim, half, pitch, tw, th, W, H, K, q, r, row0, col0, lane, min_valid, lm;
+    int ref_pitch, ref_dx, ref_dy;  // where the reference subset is read (SolveArgs)
     // the TMA tile (warp-uniform)
     int tx0, ty0;
     bool tile_ok, tile_on;
@@ -854,7 +855,7 @@ struct WarpSolver {
             const int rr = k / 6, cc = k % 6;
             Hr[k] = Hs21[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
         }
-        ref_base = (cy - half) * pitch + (cx - half);
+        ref_base = (cy - half + ref_dy) * ref_pitch + (cx - half + ref_dx);
         refok = 0;
         int g = 0;
         int row = row0, col = col0;
@@ -862,7 +863,7 @@ struct WarpSolver {
         for (int k = 0; k < K; ++k) {
             const int i = lane + 32 * k;
             if (i < n) {
-                const int idx = ref_base + row * pitch + col;
+                const int idx = ref_base + row * ref_pitch + col;
                 const float I = __ldg(refI + idx);
                 const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
                 if (I < kGhost)
@@ -1304,7 +1305,7 @@ struct WarpSolver {
             const int v = -15 + 2 * (idx / 16), u = -15 + 2 * (idx % 16);
             auto sample_at = [&](int i, float& rr, float& dd) {
                 const int row = i / dim, col = i - (i / dim) * dim;
-                const float rv = __ldg(refI + ref_base + row * pitch + col);
+                const float rv = __ldg(refI + ref_base + row * ref_pitch + col);
                 if (rv < kGhost) return false;
                 const int x = cx + (col - half) + u, y = cy + (row - half) + v;
                 if (x < 4 || x > W - 5 || y < 4 || y > H - 5) return false;
@@ -1368,7 +1369,8 @@ template <bool SIX>
 __device__ __forceinline__ void solver_setup(WarpSolver<SIX>& s, unsigned char* smem, const StagedLayout& L,
                                              const CUtensorMap* tmap, const float* refI, const float* refGx,
                                              const float* refGy, const float* defI, int* err, int n, int dim,
-                                             int pitch, int tw, int th, int W, int H, int min_valid, int lm) {
+                                             int pitch, int tw, int th, int W, int H, int min_valid, int lm,
+                                             int ref_pitch, int ref_dx, int ref_dy) {
     const int lane = threadIdx.x & 31;
     s.bar = reinterpret_cast<uint64_t*>(smem);
     s.Hr = reinterpret_cast<double*>(smem + 64);
@@ -1388,6 +1390,9 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX>& s, unsigned char* 
     s.dim = dim;
     s.half = dim / 2;
     s.pitch = pitch;
+    s.ref_pitch = ref_pitch > 0 ? ref_pitch : pitch;
+    s.ref_dx = ref_dx;
+    s.ref_dy = ref_dy;
     s.tw = tw;
     s.th = th;
     s.W = W;
@@ -1416,7 +1421,7 @@ __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtens
     extern __shared__ __align__(128) unsigned char smem[];
     WarpSolver<SIX> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
-                 a.tile_h, a.W, a.H, a.min_valid, a.lm);
+                 a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
     const int lane = s.lane, dim = s.dim, half = s.half;
     const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
     int* const n_deferred = a.queue + 2;
@@ -1486,7 +1491,7 @@ __global__ void __launch_bounds__(32, 1) rescue_kernel(const __grid_constant__ C
     extern __shared__ __align__(128) unsigned char smem[];
     WarpSolver<SIX> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
-                 a.tile_h, a.W, a.H, a.min_valid, a.lm);
+                 a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
     const int lane = s.lane, dim = s.dim, half = s.half;
     const int ntasks = *(volatile const int*)(a.queue + 2);
     int* const queue = a.queue + 1;
@@ -1668,6 +1673,9 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     const StagedLayout SL = staged_layout(a.n, tw, th);
     const bool staged_ok = ((a.n + 31) >> 5) <= kFastMaxPerLane && SL.bytes <= kFastMaxSmem;
     a.general_all = staged_ok ? 0 : 1;
+    // reference planes of another frame are read by the staged solver only
+    const bool own_ref = (a.ref_pitch > 0 && a.ref_pitch != a.pitch) || a.ref_dx != 0 || a.ref_dy != 0;
+    if (own_ref && !staged_ok) return cudaErrorInvalidValue;
     return six ? launch_passes<true>(tmap, a, SL, staged_ok, grid_blocks, smem, st)
                : launch_passes<false>(tmap, a, SL, staged_ok, grid_blocks, smem, st);
 }

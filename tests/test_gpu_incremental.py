@@ -1,0 +1,105 @@
+"""IncrementalSession on the device against the same session over the CPU
+restatement (include/semper/incremental.hpp; tests/integration/
+test_incremental.cpp of the reference for the contracts checked here).
+
+Both sessions run the shared session logic; their solves, reference
+adoptions and packing agree bit for bit, so every frame's points, return
+code and frame info must be identical.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import semper_b200 as sb
+
+pytestmark = pytest.mark.gpu
+
+COUNT_SLOTS = [0, 1, 2, 3, 4, 5, 6, 7, 8, 15, 16, 19, 20, 21, 22, 23]
+
+
+def sequence(n=256, frames=6, seed=31):
+    ref = sb.speckle(n, n, seed)
+    out = []
+    for t in range(1, frames + 1):
+        a = 0.004 * t
+        w = sb.warp_block(cx=n / 2, cy=n / 2, u0=0.9 * t, v0=-0.5 * t, a=(a, 0.0, 0.0, -0.5 * a))
+        out.append(sb.speckle(n, n, seed, w, 1.0, 100 + t))
+    return ref, out
+
+
+def run_both(ref, frames, prm_list, interval, mask=None):
+    n = ref.shape[0]
+    dev = sb.Incremental()
+    ora = oracle.IncrementalOracle()
+    assert dev.init(ref, sb.params(*prm_list), interval, mask=mask) == 0
+    assert ora.init(ref, [*prm_list[0], prm_list[1], prm_list[2], prm_list[3], 0], interval, mask=mask) == 0
+    cap = (n // prm_list[1]) ** 2 * 8
+    rows = []
+    for f in frames:
+        d = dev.process(f, cap)
+        o = ora.process(f, cap)
+        rows.append((d, o))
+    return rows
+
+
+def assert_same(d, o):
+    rc, pts, met, info = d
+    orc, opts, omet, oinfo = o
+    assert rc == orc
+    assert np.array_equal(pts, opts)
+    assert np.array_equal(met[COUNT_SLOTS], omet[COUNT_SLOTS])
+    got = [info.reference_frame, info.reference_updated, info.tracked_points, info.frame0_points,
+           info.taylor_fallbacks, info.lost_this_frame]
+    assert got == oinfo.tolist()
+
+
+@pytest.mark.parametrize("interval", [0, 1, 3])
+def test_session_matches_restatement(interval):
+    ref, frames = sequence()
+    rows = run_both(ref, frames, ((16, 16, 224, 224), 8, 21, 21), interval)
+    for d, o in rows:
+        assert_same(d, o)
+        assert d[0] > 400
+    updated = [d[3].reference_updated for d, _ in rows]
+    if interval == 0:
+        assert not any(updated)
+    elif interval == 1:
+        assert all(updated)
+    else:
+        assert updated[2] and updated[5]
+
+
+def test_masked_session_matches_restatement():
+    ref, frames = sequence(seed=17)
+    yy, xx = np.mgrid[0:256, 0:256]
+    mask = np.full((256, 256), 255, np.uint8)
+    mask[(xx - 140) ** 2 + (yy - 120) ** 2 < 30 ** 2] = 0
+    rows = run_both(ref, frames[:4], ((16, 16, 224, 224), 8, 21, 21), 2, mask=mask)
+    for d, o in rows:
+        assert_same(d, o)
+
+
+def test_interval_zero_is_a_fixed_reference_run():
+    ref, frames = sequence(frames=3)
+    prm = sb.params((16, 16, 224, 224), 8, 21, 21)
+    inc = sb.Incremental()
+    assert inc.init(ref, prm, 0) == 0
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    for f in frames:
+        rc, pts, _met, _info = inc.process(f, 28 * 28 * 8)
+        rc2, pts2, _m2 = e.run(f, prm)
+        assert rc == rc2 and np.array_equal(pts, pts2)
+
+
+def test_first_frame_is_a_fixed_reference_run():
+    ref, frames = sequence(frames=1)
+    prm = sb.params((16, 16, 224, 224), 8, 21, 21)
+    inc = sb.Incremental()
+    assert inc.init(ref, prm, 1) == 0
+    rc, pts, _met, info = inc.process(frames[0], 28 * 28 * 8)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    rc2, pts2, _m2 = e.run(frames[0], prm)
+    assert rc == rc2 and np.array_equal(pts, pts2)
+    assert info.reference_updated == 1 and info.frame0_points == 625
