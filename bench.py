@@ -46,8 +46,13 @@ sys.path.insert(0, os.path.join(REPO, "semper-dic-engine_b200"))
 
 FLOP_PER_PIXEL_ITER = {False: 117, True: 181}  # 4x4 bicubic / 6x6 Keys, per subset pixel per IC-GN iteration
 METRIC = "DIC grid points/sec on 1 B200 at <=0.01 px vs FP64; learned vs lattice seeding"
-WORKLOAD = ("cfg1: 4096x4096 uint8 speckle, u=0.005x+2sin(2pi y/256), v=-0.003y+1.5sin(2pi x/384), "
-            "noise sigma 2, step 4, subset 31, strain window 31, 4x4 bicubic, fixed reference (frames 2+)")
+WORKLOADS = {
+    "cfg1": ("cfg1: 4096x4096 uint8 speckle, u=0.005x+2sin(2pi y/256), v=-0.003y+1.5sin(2pi x/384), "
+             "noise sigma 2, step 4, subset 31, strain window 31, 4x4 bicubic, fixed reference (frames 2+)"),
+    "cfg4-plain": ("target settings: 4096x4096 uint8 speckle under the cfg1 field, noise sigma 2, step 8, "
+                   "subset 41, strain window 41, 4x4 bicubic, fixed reference (frames 2+)"),
+}
+WORKLOAD = WORKLOADS["cfg1"]
 
 
 def _env_int(k, d):
@@ -189,6 +194,21 @@ def run_reference(args, rank):
     return 0
 
 
+def aggregate(points, ms_per_step, steps, dist=None, device="cpu"):
+    """Whole-job throughput of independent replicas: every rank's points over
+    the slowest rank's time (max over ranks), summed over ranks. Returns
+    (points/s, slowest ms per step)."""
+    import torch
+
+    ms_t = torch.tensor([ms_per_step], device=device, dtype=torch.float64)
+    pts_t = torch.tensor([points], device=device, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(pts_t, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_t.item())
+    return float(pts_t.item()) / steps / (ms_max / 1000.0), ms_max
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
 
@@ -203,7 +223,9 @@ def run_b200(args, rank, world, local_rank):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    ref, dfm, prm, warp = sb.config_pair(1, size=args.size, pair=rank)
+    cfg = 4 if args.workload == "cfg4-plain" else 1
+    workload = WORKLOADS[args.workload]
+    ref, dfm, prm, warp = sb.config_pair(cfg, size=args.size, pair=rank)
     H, W = ref.shape
     grid_nodes = (prm.rect_w // prm.step) * (prm.rect_h // prm.step)
     capacity = grid_nodes * 8
@@ -244,13 +266,7 @@ def run_b200(args, rank, world, local_rank):
     if dist:
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / args.steps
-    ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    pts_t = torch.tensor([pts], device="cuda", dtype=torch.float64)
-    if dist:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(pts_t, op=dist.ReduceOp.SUM)
-    ms_max = float(ms_t.item())
-    value = float(pts_t.item()) / args.steps / (ms_max / 1000.0)
+    value, ms_max = aggregate(pts, ms, args.steps, dist, "cuda")
 
     # e2e: public C ABI, frame in pinned host memory, points read back
     h_frame = torch.from_numpy(dfm).pin_memory()
@@ -294,12 +310,12 @@ def run_b200(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD if args.size == 4096 else f"{WORKLOAD} [resized to {W}x{H}]",
+            "config": {"workload": workload if args.size == 4096 else f"{workload} [resized to {W}x{H}]",
                        "image": [W, H], "grid_nodes": grid_nodes,
                        "attempted": int(met[0]), "points_per_step": rc,
                        "parallelism": f"replicas x{world} (independent frame pairs)",
-                       "l2": "inputs larger than L2: reference planes 201 MB + Hessian pool 177 MB + "
-                             "deformed plane 67 MB per step"},
+                       "l2": f"inputs larger than L2: reference planes {12 * W * H / 1e6:.0f} MB + Hessian pool "
+                             f"{177 * grid_nodes / 1e6:.0f} MB + deformed planes {12 * W * H / 1e6:.0f} MB per step"},
             "frames_per_s": 1000.0 / ms_max * world,
             "attempted_points_per_s": int(met[0]) * world / (ms_max / 1000.0),
             "first_frame_ms": round(first_ms, 2),
@@ -327,6 +343,63 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
+def run_cfg3(args, rank):
+    """cfg3 (incremental DIC), a bounded sample: one 2048x2048 sequence under a
+    monotone uniaxial stretch (25 % over 128 frames) plus a rigid rotation
+    (30 deg over 128 frames), noise sigma 1.5, subset 21, step 6, window 21,
+    through the public C ABI (semper_incremental_process). Warm-up frames are
+    solved but not timed; frames/s and points/s over the timed frames."""
+    if rank != 0:
+        return 0
+    import math
+
+    import torch
+
+    import semper_b200 as sb
+
+    n = args.size if args.size != 4096 else 2048
+    total = args.warmup + args.steps
+    ref = sb.speckle(n, n, 3000)
+    frames = []
+    for t in range(1, total + 1):
+        th, s = math.radians(30.0) * t / 128.0, 0.25 * t / 128.0
+        a = (math.cos(th) * (1 + s) - 1, -math.sin(th), math.sin(th) * (1 + s), math.cos(th) - 1)
+        frames.append(sb.speckle(n, n, 3000, sb.warp_block(cx=n / 2, cy=n / 2, a=a), 1.5, 4000 + t))
+    m = n // 8
+    prm = sb.params((m, m, n - 2 * m, n - 2 * m), 6, 21, 21)
+    cap = ((n - 2 * m) // 6) ** 2 * 8
+    inc = sb.Incremental()
+    assert inc.init(ref, prm, args.interval) == 0
+    ms, pts, updates = [], [], 0
+    with ClockSampler(0) as clk:
+        for i, f in enumerate(frames):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc, _out, _met, info = inc.process(f, cap)
+            dt = time.perf_counter() - t0
+            assert rc > 0, rc
+            if i >= args.warmup:
+                ms.append(1000 * dt)
+                pts.append(rc)
+                updates += info.reference_updated
+    mean_ms = statistics.mean(ms)
+    line = {
+        "metric": METRIC, "value": sum(pts) / (sum(ms) / 1000.0), "unit": "points/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"cfg3 sample: one {n}x{n} sequence, stretch 25 % + rotation 30 deg over 128 frames, "
+                               f"noise 1.5, subset 21, step 6, window 21, update_interval {args.interval}, "
+                               f"frames {args.warmup + 1}..{total} timed after {args.warmup} warm-up frames",
+                   "frames_timed": len(ms), "reference_updates": updates, "points_per_frame": statistics.mean(pts)},
+        "frames_per_s": 1000.0 / mean_ms,
+        "e2e": {"value": sum(pts) / (sum(ms) / 1000.0), "unit": "points/s", "h2d_bytes_per_step": n * n,
+                "d2h_bytes_per_step": int(statistics.mean(pts)) * 32},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -336,6 +409,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", type=int, default=4096,
                     help="image edge (default 4096, the benchmark workload; smaller sizes are for profiling)")
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg4-plain", "cfg3"],
+                    help="cfg1 (the headline line), cfg4-plain (the target settings), cfg3 (incremental sample)")
+    ap.add_argument("--interval", type=int, default=1, help="cfg3: the session's update_interval")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)
@@ -343,6 +419,8 @@ def main():
     local_rank = _env_int("LOCAL_RANK", 0)
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.workload == "cfg3":
+        return run_cfg3(args, rank)
     return run_b200(args, rank, world, local_rank)
 
 
