@@ -87,6 +87,11 @@ struct IncBackend {
             }
         return pack_field(grid, g.gridW, g.gridH, g.step, window, out, capacity).valid_count;
     }
+    semper_inc::Rect warp_mask(const std::vector<uint8_t>& mask0, int W, int H, const semper_inc::GridGeom& g,
+                               const semper_inc::MaskWarpPlan& p, std::vector<uint8_t>& out) {
+        semper_inc::scatter_mask_host(mask0, W, H, g, p, out);
+        return semper_inc::bounding_rect(out, W, H);
+    }
     // match_anchor (incremental_math.cpp:238-276) on the kept frame.
     bool match_anchor(const semper_inc::CoastAnchor& a, int subset, bool six, float gx, float gy, float max_shift,
                       float& x, float& y, float& corr) {

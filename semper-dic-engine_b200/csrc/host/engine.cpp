@@ -28,6 +28,7 @@
 #include "../kernels/icgn.cuh"
 #include "../kernels/mesh.cuh"
 #include "../kernels/prep.cuh"
+#include "../kernels/incmask.cuh"
 #include "../kernels/strain.cuh"
 #include "geometry.hpp"
 
@@ -432,6 +433,11 @@ struct Engine::Impl {
     DevBuf<dic_result> aRes;
     DevBuf<int> aQ;
 
+    // the material-mask warp of incremental DIC
+    DevBuf<uint8_t> mMask0, mOut, mTmp;
+    DevBuf<float> mU, mV;
+    DevBuf<int> mBox;
+
     void prepare_deformed(const uint8_t* d_def) {
         const size_t n = (size_t)pitch() * E.H_;
         dI.ensure(n);
@@ -515,15 +521,10 @@ int Engine::adopt_last_deformed(const uint8_t* mask) {
     if (mask) {
         // Ghost Wall on the adopted frame: the gradients stay those of the
         // real intensities (stamp after prepare, reference_cache.cpp:95-96).
-        const int P = (W_ + 3) & ~3;
-        const size_t n = (size_t)P * H_;
-        std::vector<float> plane(n);
-        check(cudaMemcpyAsync(plane.data(), I.rI.p, n * 4, cudaMemcpyDeviceToHost, stream_), "D2H plane");
-        check(cudaStreamSynchronize(stream_), "sync");
-        for (int y = 0; y < H_; ++y)
-            for (int x = 0; x < W_; ++x)
-                if (mask[(size_t)y * W_ + x] < 128) plane[(size_t)y * P + x] = -10.0f;
-        check(cudaMemcpyAsync(I.rI.p, plane.data(), n * 4, cudaMemcpyHostToDevice, stream_), "H2D plane");
+        const size_t n = (size_t)W_ * H_;
+        I.mOut.ensure(std::max(I.mOut.n, n));
+        check(cudaMemcpyAsync(I.mOut.p, mask, n, cudaMemcpyHostToDevice, stream_), "H2D mask");
+        I.launched(1, dic::launch_stamp_ghost(I.rI.p, W_, H_, (W_ + 3) & ~3, I.mOut.p, stream_), "ghost stamp");
         check(cudaStreamSynchronize(stream_), "sync");
     }
     I.grid_valid = false;
@@ -549,6 +550,41 @@ int Engine::run(const uint8_t* def_gray, const uint8_t* mask, Params p, float* o
 }
 
 int check_params(Params& p, int width, int height) { return validate_params(p, width, height); }
+
+int Engine::warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, int rect_x, int rect_y, int step,
+                      const float* U, const float* V, int X0, int X1, int Y0, int Y1, int per_px, uint8_t* out,
+                      int box[4]) {
+    Impl& I = *impl_;
+    if (!mask0 || !U || !V || !out || W <= 0 || H <= 0 || gridW <= 0 || gridH <= 0 || step <= 0) return -3;
+    cudaStream_t st = stream_;
+    const size_t n = (size_t)W * H, ng = (size_t)gridW * gridH;
+    I.mMask0.ensure(std::max(I.mMask0.n, n));
+    I.mOut.ensure(std::max(I.mOut.n, n));
+    I.mTmp.ensure(std::max(I.mTmp.n, n));
+    I.mU.ensure(std::max(I.mU.n, ng));
+    I.mV.ensure(std::max(I.mV.n, ng));
+    I.mBox.ensure(4);
+    check(cudaMemcpyAsync(I.mMask0.p, mask0, n, cudaMemcpyHostToDevice, st), "H2D material mask");
+    check(cudaMemcpyAsync(I.mU.p, U, ng * 4, cudaMemcpyHostToDevice, st), "H2D U");
+    check(cudaMemcpyAsync(I.mV.p, V, ng * 4, cudaMemcpyHostToDevice, st), "H2D V");
+    const dic::MaskField f{gridW, gridH, rect_x, rect_y, step, I.mU.p, I.mV.p};
+    I.launched(1, dic::launch_warp_mask(I.mMask0.p, W, H, X0, X1, Y0, Y1, per_px, f, I.mOut.p, st), "mask warp");
+    I.launched(2, dic::launch_close3x3(I.mOut.p, I.mTmp.p, W, H, st), "mask close");
+    I.launched(2, dic::launch_mask_bbox(I.mOut.p, W, H, I.mBox.p, st), "mask box");
+    int b[4] = {0, 0, 0, 0};
+    check(cudaMemcpyAsync(out, I.mOut.p, n, cudaMemcpyDeviceToHost, st), "D2H mask");
+    check(cudaMemcpyAsync(b, I.mBox.p, sizeof(b), cudaMemcpyDeviceToHost, st), "D2H box");
+    check(cudaStreamSynchronize(st), "sync");
+    if (b[2] < 0) {
+        box[0] = box[1] = box[2] = box[3] = 0;
+    } else {
+        box[0] = b[0];
+        box[1] = b[1];
+        box[2] = b[2] - b[0] + 1;
+        box[3] = b[3] - b[1] + 1;
+    }
+    return 0;
+}
 int vsg_window_nodes(int step, int window) { return vsg_window_node_count(step, window); }
 
 int Engine::pack_field(int gW, int gH, int rect_x, int rect_y, int step, int window, const float* u, const float* v,
@@ -1301,6 +1337,13 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         int dropped_outlier = 0, dropped_post = 0;
         const int valid_count = strain_pack(gW, gH, params.rect_x, params.rect_y, params.step, params.strain_window,
                                             d_out_p, capacity, dropped_outlier, dropped_post);
+        if (capture) {
+            capture->median_valid.resize(NG);
+            check(cudaMemcpyAsync(capture->median_valid.data(), valid.p, NG, cudaMemcpyDeviceToHost, st),
+                  "D2H median flags");
+            capture->median_rejected = dropped_outlier;
+            sync();
+        }
         const double ms_strain = ms_since(t_strain);
         ticker.stop();
         if (progress) {

@@ -64,6 +64,10 @@ struct Capture {
     int gridW = 0, gridH = 0, rect_x = 0, rect_y = 0, step = 0, attempted = 0;
     std::vector<float> u, v, ux, uy, vx, vy, corr;
     std::vector<uint8_t> solved;
+    // the nodes holding a result (solved, corr >= 0) that pass the
+    // displacement median test of the packing, and how many it rejected
+    std::vector<uint8_t> median_valid;
+    int median_rejected = 0;
 };
 
 // Timings of one solve's device phases, measured with CUDA events on the
@@ -131,6 +135,15 @@ public:
     // sits at (ax, ay), solved in NO_SEARCH mode on the deformed frame of the
     // last run from the guess (gu, gv) of its displacement.
     PatchSolve solve_patch(const uint8_t* patch, int size, int ax, int ay, float gu, float gv, int subset, bool six);
+
+    // warp_material_mask's scatter and close (incremental_math.cpp:371-447)
+    // on the device: every material pixel (mask0 >= 128) of the window
+    // [X0, X1] x [Y0, Y1] sends per_px x per_px samples X to X + U(X), U the
+    // filled field of the grid; then a 3x3 close. out (host, W x H) receives
+    // the mask; box = {x, y, w, h} of its nonzero pixels (all 0 if none).
+    int warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, int rect_x, int rect_y, int step,
+                  const float* U, const float* V, int X0, int X1, int Y0, int Y1, int per_px, uint8_t* out,
+                  int box[4]);
 
     void request_cancel() { h_cancel_[0] = 1; }
     void clear_cancel() { h_cancel_[0] = 0; }

@@ -4,6 +4,7 @@
 
 #include <cmath>
 #include <cstring>
+#include <stdexcept>
 
 #include "incremental_core.hpp"
 
@@ -71,6 +72,8 @@ struct DeviceBackend {
         cap->vy = std::move(c.vy);
         cap->corr = std::move(c.corr);
         cap->solved = std::move(c.solved);
+        cap->median_valid = std::move(c.median_valid);
+        cap->median_rejected = c.median_rejected;
         return rc;
     }
     int adopt(const uint8_t* mask) { return e.adopt_last_deformed(mask); }
@@ -78,6 +81,15 @@ struct DeviceBackend {
              const std::vector<float>& corr, const std::vector<unsigned char>& solved, float* out, int capacity) {
         return e.pack_field(g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, window, u.data(), v.data(), corr.data(),
                             solved.data(), out, capacity);
+    }
+    semper_inc::Rect warp_mask(const std::vector<uint8_t>& mask0, int W, int H, const semper_inc::GridGeom& g,
+                               const semper_inc::MaskWarpPlan& p, std::vector<uint8_t>& out) {
+        out.resize((size_t)W * H);
+        int box[4] = {0, 0, 0, 0};
+        if (e.warp_mask(mask0.data(), W, H, g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, p.U.data(), p.V.data(),
+                        p.X0, p.X1, p.Y0, p.Y1, p.per_px, out.data(), box) != 0)
+            throw std::runtime_error("mask warp");
+        return semper_inc::Rect{box[0], box[1], box[2], box[3]};
     }
     bool match_anchor(const semper_inc::CoastAnchor& a, int subset, bool six, float gx, float gy, float max_shift,
                       float& x, float& y, float& corr) {

@@ -64,6 +64,10 @@ struct SolveCapture {
     int gridW = 0, gridH = 0, rect_x = 0, rect_y = 0, step = 0, attempted = 0;
     std::vector<float> u, v, ux, uy, vx, vy, corr;
     std::vector<unsigned char> solved;
+    // optional: the flags of the solve's own displacement median test over
+    // the same nodes (the packing ran it already), and its rejection count
+    std::vector<unsigned char> median_valid;
+    int median_rejected = 0;
 };
 
 inline float median_inplace(std::vector<float>& v) {
@@ -153,6 +157,12 @@ inline NodeField node_field_from_capture(const SolveCapture& cap, int* rejected 
         f.vy[i] = cap.vy[i];
         f.corr[i] = cap.corr[i];
         f.valid[i] = 1;
+    }
+    if (cap.median_valid.size() == n) {
+        // the same test on the same nodes, already run by the solve
+        for (size_t i = 0; i < n; ++i) f.valid[i] = f.valid[i] && cap.median_valid[i] ? 1 : 0;
+        if (rejected) *rejected = cap.median_rejected;
+        return f;
     }
     const int dropped = reject_outliers(f.gridW, f.gridH, f.u, f.v, f.valid);
     if (rejected) *rejected = dropped;
@@ -521,6 +531,7 @@ struct ContinuousField {
 // the dilation and the erosion.
 inline void close3x3(std::vector<uint8_t>& m, int W, int H) {
     std::vector<uint8_t> d((size_t)W * H);
+#pragma omp parallel for schedule(static)
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
             uint8_t v = 0;
@@ -535,6 +546,7 @@ inline void close3x3(std::vector<uint8_t>& m, int W, int H) {
                 }
             d[(size_t)y * W + x] = v;
         }
+#pragma omp parallel for schedule(static)
     for (int y = 0; y < H; ++y)
         for (int x = 0; x < W; ++x) {
             uint8_t v = 255;
@@ -551,41 +563,53 @@ inline void close3x3(std::vector<uint8_t>& m, int W, int H) {
         }
 }
 
-// warp_material_mask (incremental_math.cpp:371-447): every frame-0 material
-// sample X (per_px x per_px per pixel) lands at X + U(X); the landed pixels
-// are closed with a 3x3 kernel. All zero when no node is valid.
-inline std::vector<uint8_t> warp_material_mask(const std::vector<uint8_t>& mask0, int W, int H, const GridGeom& geom,
-                                               const std::vector<float>& U_in, const std::vector<float>& V_in,
-                                               const std::vector<unsigned char>& valid, int margin_px) {
-    std::vector<uint8_t> out((size_t)W * H, 0);
-    if (geom.gridW <= 0 || geom.gridH <= 0 || geom.step <= 0) return out;
-    std::vector<float> U(U_in), V(V_in);
-    if (!fill_field(geom.gridW, geom.gridH, U, V, valid)) return out;
-    const ContinuousField field{geom, U, V};
+// warp_material_mask (incremental_math.cpp:371-447), in two steps. The plan:
+// the filled field, the samples per pixel and the frame-0 window; false when
+// no node is valid or the window is empty (the warped mask is then empty).
+struct MaskWarpPlan {
+    std::vector<float> U, V;  // filled over the grid
+    int per_px = 2;
+    int X0 = 0, X1 = -1, Y0 = 0, Y1 = -1;
+};
+
+inline bool plan_mask_warp(const GridGeom& geom, const std::vector<float>& U_in, const std::vector<float>& V_in,
+                           const std::vector<unsigned char>& valid, int W, int H, int margin_px, MaskWarpPlan& p) {
+    if (geom.gridW <= 0 || geom.gridH <= 0 || geom.step <= 0) return false;
+    p.U = U_in;
+    p.V = V_in;
+    if (!fill_field(geom.gridW, geom.gridH, p.U, p.V, valid)) return false;
     double stretch = 1.0;
     for (int gy = 0; gy < geom.gridH; ++gy)
         for (int gx = 0; gx < geom.gridW; ++gx) {
             const size_t i = (size_t)gy * geom.gridW + gx;
             const size_t ix = gx + 1 < geom.gridW ? i + 1 : i;
             const size_t iy = gy + 1 < geom.gridH ? i + geom.gridW : i;
-            const double ux = (U[ix] - U[i]) / geom.step, uy = (U[iy] - U[i]) / geom.step;
-            const double vx = (V[ix] - V[i]) / geom.step, vy = (V[iy] - V[i]) / geom.step;
+            const double ux = (p.U[ix] - p.U[i]) / geom.step, uy = (p.U[iy] - p.U[i]) / geom.step;
+            const double vx = (p.V[ix] - p.V[i]) / geom.step, vy = (p.V[iy] - p.V[i]) / geom.step;
             stretch = std::max(stretch, std::max(std::abs(1 + ux) + std::abs(uy), std::abs(vx) + std::abs(1 + vy)));
         }
-    const int per_px = std::min(kIncMaskMaxSamplesPerPx, std::max(2, (int)std::ceil(stretch / 0.7)));
-    const double hs = 1.0 / per_px;
-    const int X0 = std::max(0, geom.rect_x - margin_px);
-    const int X1 = std::min(W - 1, geom.rect_x + (geom.gridW - 1) * geom.step + margin_px);
-    const int Y0 = std::max(0, geom.rect_y - margin_px);
-    const int Y1 = std::min(H - 1, geom.rect_y + (geom.gridH - 1) * geom.step + margin_px);
-    if (X0 > X1 || Y0 > Y1) return out;
+    p.per_px = std::min(kIncMaskMaxSamplesPerPx, std::max(2, (int)std::ceil(stretch / 0.7)));
+    p.X0 = std::max(0, geom.rect_x - margin_px);
+    p.X1 = std::min(W - 1, geom.rect_x + (geom.gridW - 1) * geom.step + margin_px);
+    p.Y0 = std::max(0, geom.rect_y - margin_px);
+    p.Y1 = std::min(H - 1, geom.rect_y + (geom.gridH - 1) * geom.step + margin_px);
+    return p.X0 <= p.X1 && p.Y0 <= p.Y1;
+}
+
+// The scatter: every frame-0 material sample X (per_px x per_px per pixel of
+// the window) lands at X + U(X); then the 3x3 close.
+inline void scatter_mask_host(const std::vector<uint8_t>& mask0, int W, int H, const GridGeom& geom,
+                              const MaskWarpPlan& p, std::vector<uint8_t>& out) {
+    out.assign((size_t)W * H, 0);
+    const ContinuousField field{geom, p.U, p.V};
+    const double hs = 1.0 / p.per_px;
 #pragma omp parallel for schedule(static)
-    for (int sy = Y0; sy <= Y1; ++sy) {
+    for (int sy = p.Y0; sy <= p.Y1; ++sy) {
         const uint8_t* mrow = mask0.data() + (size_t)sy * W;
-        for (int sx = X0; sx <= X1; ++sx) {
+        for (int sx = p.X0; sx <= p.X1; ++sx) {
             if (mrow[sx] < 128) continue;
-            for (int b = 0; b < per_px; ++b)
-                for (int a = 0; a < per_px; ++a) {
+            for (int b = 0; b < p.per_px; ++b)
+                for (int a = 0; a < p.per_px; ++a) {
                     const double X = sx - 0.5 + (a + 0.5) * hs, Y = sy - 0.5 + (b + 0.5) * hs;
                     double u, v;
                     field.eval(X, Y, u, v);
@@ -597,6 +621,15 @@ inline std::vector<uint8_t> warp_material_mask(const std::vector<uint8_t>& mask0
         }
     }
     close3x3(out, W, H);
+}
+
+inline std::vector<uint8_t> warp_material_mask(const std::vector<uint8_t>& mask0, int W, int H, const GridGeom& geom,
+                                               const std::vector<float>& U_in, const std::vector<float>& V_in,
+                                               const std::vector<unsigned char>& valid, int margin_px) {
+    std::vector<uint8_t> out;
+    MaskWarpPlan p;
+    if (!plan_mask_warp(geom, U_in, V_in, valid, W, H, margin_px, p)) return std::vector<uint8_t>((size_t)W * H, 0);
+    scatter_mask_host(mask0, W, H, geom, p, out);
     return out;
 }
 
@@ -667,6 +700,10 @@ inline int64_t max_strain_window(const IncParams& p) {
 //                                                   pack_full_field_output
 //   bool match_anchor(const CoastAnchor&, subset, six, gx, gy, max_shift, x, y, corr)
 //                                                   match_anchor on the kept frame
+//   Rect warp_mask(mask0, W, H, const GridGeom&, const MaskWarpPlan&, out)
+//                                                   the scatter and close of
+//                                                   warp_material_mask; returns
+//                                                   the bounding box of `out`
 template <class B>
 class IncrementalCore {
 public:
@@ -943,9 +980,14 @@ private:
         r.alive = valid;
         const int half = params_.subset_size / 2;
         const int margin = (kIncMaskExtrapCells + 1) * grid0_.step + half;
-        r.mask_k = warp_material_mask(material_mask0_, width_, height_, grid0_, r.Ubase, r.Vbase, r.alive, margin);
+        MaskWarpPlan plan;
+        Rect bb;
+        if (plan_mask_warp(grid0_, r.Ubase, r.Vbase, r.alive, width_, height_, margin, plan)) {
+            bb = b_.warp_mask(material_mask0_, width_, height_, grid0_, plan, r.mask_k);
+        } else {
+            r.mask_k.assign((size_t)width_ * height_, 0);
+        }
         r.params_k = params_;
-        const Rect bb = bounding_rect(r.mask_k, width_, height_);
         float min_x = 1e30f, min_y = 1e30f, max_x = -1e30f, max_y = -1e30f;
         for (int j = 0; j < grid0_.gridH; ++j)
             for (int i = 0; i < grid0_.gridW; ++i) {
