@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <type_traits>
 
 #include "common.cuh"
 #include "dic_types.h"
@@ -801,7 +802,7 @@ StagedLayout staged_layout(int n, int tw, int th) {
     return L;
 }
 
-template <bool SIX>
+template <bool SIX, class Mask = uint64_t>
 struct WarpSolver {
     // this warp's shared memory
     uint64_t* bar;
@@ -828,7 +829,7 @@ struct WarpSolver {
     // the task
     int cx, cy, ref_base, ghost;
     float mref, iref, lo_x, hi_x, lo_y, hi_y;
-    uint64_t refok;
+    Mask refok;
 
     __device__ __forceinline__ void advance(int& row, int& col) const {
         col += r;
@@ -869,7 +870,7 @@ struct WarpSolver {
                 if (I < kGhost)
                     ++g;
                 else
-                    refok |= 1ull << k;
+                    refok |= Mask(1) << k;
                 srn[i] = (I - mref) * iref;
                 sgx[i] = gx;
                 sgy[i] = gy;
@@ -939,9 +940,8 @@ struct WarpSolver {
     // value into vals, the valid ones (inside the guard, outside the Ghost
     // Wall) flagged in `valid` and summed; returns their count. Four pixels'
     // loads are issued before their stores.
-    __device__ __forceinline__ int sample(const float Wp[6], float& sum, uint64_t& valid) {
+    __device__ __forceinline__ int sample(const float Wp[6], float& sum, Mask& valid) {
         ensure_tile(Wp);
-        const int lo_tap = SIX ? 2 : 1, hi_tap = SIX ? 3 : 2;
         float part = 0.0f;
         int cnt = 0;
         valid = 0;
@@ -963,14 +963,17 @@ struct WarpSolver {
                         const float flx = floorf(fx), fly = floorf(fy);
                         const int xi = cx + (int)flx, yi = cy + (int)fly;
                         const int lx = xi - tx0, ly = yi - ty0;
-                        if (tile_ok && lx >= lo_tap && lx + hi_tap < tw && ly >= lo_tap && ly + hi_tap < th)
+                        // a staged tile covers every sample support: ensure_tile sized it from
+                        // the warped corners, which bound every interior sample, with a pixel
+                        // of slack each side for the rounding of the corner positions
+                        if (tile_ok)
                             v[u] = SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly)
                                        : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
                         else
                             v[u] = SIX ? interp6(defI, pitch, xi, yi, fx - flx, fy - fly)
                                        : interp4(defI, pitch, xi, yi, fx - flx, fy - fly);
-                        if ((refok >> k) & 1ull) {
-                            valid |= 1ull << k;
+                        if ((refok >> k) & 1u) {
+                            valid |= Mask(1) << k;
                             part = part + v[u];
                             ++cnt;
                         }
@@ -987,11 +990,11 @@ struct WarpSolver {
         return wsum(cnt);
     }
 
-    __device__ __forceinline__ float sum_sq(float mean, uint64_t valid) const {
+    __device__ __forceinline__ float sum_sq(float mean, Mask valid) const {
         float sq = 0.0f;
 #pragma unroll 4
         for (int k = 0; k < K; ++k) {
-            if (!((valid >> k) & 1ull)) continue;
+            if (!((valid >> k) & 1u)) continue;
             const float d = vals[lane + 32 * k] - mean;
             sq = __fmaf_rn(d, d, sq);
         }
@@ -1000,13 +1003,13 @@ struct WarpSolver {
 
     // The masked iteration's own Hessian (optimization_engine.cpp:373-413),
     // FP64, into Hm; false to reject.
-    __device__ __forceinline__ bool masked_step(uint64_t valid) {
+    __device__ __forceinline__ bool masked_step(Mask valid) {
         double hp[21];
 #pragma unroll
         for (int k = 0; k < 21; ++k) hp[k] = 0.0;
         int row = row0, col = col0;
         for (int k = 0; k < K; ++k) {
-            if ((valid >> k) & 1ull) {
+            if ((valid >> k) & 1u) {
                 const int i = lane + 32 * k;
                 const float g0 = sgx[i] * iref, g1 = sgy[i] * iref;
                 const float fx = (float)(col - half), fy = (float)(row - half);
@@ -1055,7 +1058,7 @@ struct WarpSolver {
         float final_score = 1.0f;
         for (int iter = 0; iter < kIcgnMaxIter; ++iter) {
             float sum;
-            uint64_t valid;
+            Mask valid;
             const int cnt = sample(Wp, sum, valid);
             if (cnt < min_valid) return res_from(Wp, 1, 2.0f, iter);
             const bool full = cnt == n;
@@ -1075,7 +1078,7 @@ struct WarpSolver {
                 int row = row0, col = col0;
 #pragma unroll 4
                 for (int k = 0; k < K; ++k) {
-                    if ((valid >> k) & 1ull) {
+                    if ((valid >> k) & 1u) {
                         const int i = lane + 32 * k;
                         const float rn = srn[i], g0 = sgx[i] * iref, g1 = sgy[i] * iref;
                         const float fx = (float)(col - half), fy = (float)(row - half);
@@ -1147,7 +1150,7 @@ struct WarpSolver {
                 float sx = 0.0f, sy = 0.0f;
 #pragma unroll 4
                 for (int k = 0; k < K; ++k) {
-                    if ((valid >> k) & 1ull) {
+                    if ((valid >> k) & 1u) {
                         const int i = lane + 32 * k;
                         const float gx = sgx[i], gy = sgy[i];
                         sx = __fmaf_rn(gx, gx, sx);
@@ -1166,7 +1169,7 @@ struct WarpSolver {
     // evaluate_znssd (optimization_engine.cpp:467-528).
     __device__ __forceinline__ float znssd(const float Wp[6]) {
         float sum;
-        uint64_t valid;
+        Mask valid;
         const int cnt = sample(Wp, sum, valid);
         if (cnt == 0 || cnt < min_valid) return 2.0f;
         const float mean = sum / (float)cnt;
@@ -1177,7 +1180,7 @@ struct WarpSolver {
         float ep = 0.0f;
 #pragma unroll 4
         for (int k = 0; k < K; ++k) {
-            if ((valid >> k) & 1ull) {
+            if ((valid >> k) & 1u) {
                 const int i = lane + 32 * k;
                 const float rn = srn[i];
                 const float diff = full ? rn - (vals[i] - mean) * inv : rn - (vals[i] - mean) / sdev;
@@ -1365,8 +1368,8 @@ struct WarpSolver {
 
 // Set a warp's solver up for a launch: shared-memory arrays, launch
 // constants (copied out of the by-value argument block), tile state, barrier.
-template <bool SIX>
-__device__ __forceinline__ void solver_setup(WarpSolver<SIX>& s, unsigned char* smem, const StagedLayout& L,
+template <bool SIX, class Mask>
+__device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask>& s, unsigned char* smem, const StagedLayout& L,
                                              const CUtensorMap* tmap, const float* refI, const float* refGx,
                                              const float* refGy, const float* defI, int* err, int n, int dim,
                                              int pitch, int tw, int th, int W, int H, int min_valid, int lm,
@@ -1415,13 +1418,21 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX>& s, unsigned char* 
 }
 
 // The fast pass over every task: the common case, everything else deferred.
-template <bool SIX>
+// DIMC > 0: the subset size, the tile box and the pixels per lane known at
+// compile time (the launch checks they match), so the per-pixel loop
+// bookkeeping folds away; 32-bit validity masks up to 32 pixels per lane.
+template <bool SIX, int DIMC>
 __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                   const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
-    WarpSolver<SIX> s;
-    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
-                 a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+    using Mask = std::conditional_t<(DIMC > 0 && DIMC * DIMC <= 1024), uint32_t, uint64_t>;
+    constexpr int kTw = DIMC > 0 ? ((DIMC + (SIX ? 5 : 3) + 2 + 7 + 3) & ~3) : 0;
+    constexpr int kTh = DIMC > 0 ? DIMC + (SIX ? 5 : 3) + 2 + 4 : 0;
+    WarpSolver<SIX, Mask> s;
+    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
+                 DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
+                 a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+    if (DIMC > 0) s.tile_on = a.tile_w > 0;
     const int lane = s.lane, dim = s.dim, half = s.half;
     const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
     int* const n_deferred = a.queue + 2;
@@ -1489,7 +1500,7 @@ template <bool SIX>
 __global__ void __launch_bounds__(32, 1) rescue_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                        const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
-    WarpSolver<SIX> s;
+    WarpSolver<SIX, uint64_t> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
                  a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
     const int lane = s.lane, dim = s.dim, half = s.half;
@@ -1587,11 +1598,19 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
     long blocks = 1;
     cudaError_t e;
     if (staged_ok) {
-        e = cudaFuncSetAttribute(fast_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
+        // subset sizes with a compile-time kernel (the tile box must be the one it assumes)
+        int tw = 0, th = 0;
+        tile_box(a.dim, SIX ? 1 : 0, tw, th);
+        const bool box_ok = a.tile_w == 0 || (a.tile_w == tw && a.tile_h == th);
+        auto fast = fast_kernel<SIX, 0>;
+        if (box_ok && a.dim == 21) fast = fast_kernel<SIX, 21>;
+        if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31>;
+        if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41>;
+        e = cudaFuncSetAttribute(fast, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
         if (e != cudaSuccess) return e;
-        e = one_wave(fast_kernel<SIX>, SL.bytes, 0, a.n_tasks, blocks);
+        e = one_wave(fast, SL.bytes, 0, a.n_tasks, blocks);
         if (e != cudaSuccess) return e;
-        fast_kernel<SIX><<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
+        fast<<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
         e = cudaFuncSetAttribute(rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
         if (e != cudaSuccess) return e;
         e = one_wave(rescue_kernel<SIX>, SL.bytes, cap, a.n_tasks, blocks);
