@@ -760,11 +760,14 @@ __global__ void __launch_bounds__(32, 1)
 
 // ---------------------------------------------------------------------------
 // The staged solvers: one warp per subset and one warp per block, so that
-// shared memory alone sets the occupancy. Per task the warp stages its
-// reference subset in shared memory ((I - mean) / std, and the raw gradients,
-// which the texture check needs as they are), so the iterations read only
-// shared memory: the reference subset, the TMA tile of the deformed image and
-// the sampled values. Validity and Ghost Wall flags are per-lane bit masks
+// shared memory alone sets the occupancy. The deformed image is read from a
+// TMA tile in shared memory and the sampled values are kept there. With STAGE
+// the warp also stages its reference subset per task ((I - mean) / std, and
+// the raw gradients, which the texture check needs as they are), so that the
+// iterations read only shared memory (the rescue pass); without it the
+// reference is read from the planes, normalised the same way, and a warp
+// takes about half the shared memory (the fast pass, where occupancy pays
+// more than the staging). Validity and Ghost Wall flags are per-lane bit masks
 // (pixel lane + 32k is bit k); the tile state is warp-uniform registers.
 // Arithmetic and summation order are those of solve_kernel (and of the CPU
 // restatement), so every kernel gives the same bits.
@@ -776,7 +779,7 @@ __global__ void __launch_bounds__(32, 1)
 //
 // Shared memory per warp: the TMA barrier at 0, the whole-subset step matrix
 // (36 doubles) at 64, the masked-iteration step matrix at 352, the tile at
-// off_tile, then vals[n], rn[n], gx[n], gy[n].
+// off_tile, then vals[n] and (STAGE) rn[n], gx[n], gy[n].
 constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets go to solve_kernel
 constexpr int kFastMaxSmem = 227 * 1024;
 
@@ -785,24 +788,28 @@ struct StagedLayout {
     int bytes;  // per warp, a multiple of 128
 };
 
-StagedLayout staged_layout(int n, int tw, int th) {
+// stage false: no staged reference subset (the solver reads the planes)
+StagedLayout staged_layout(int n, int tw, int th, bool stage = true) {
     StagedLayout L;
     L.off_tile = 640;
     int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
     const int arr = (n * 4 + 15) & ~15;
     L.off_vals = p;
     p += arr;
-    L.off_rn = p;
-    p += arr;
-    L.off_gx = p;
-    p += arr;
-    L.off_gy = p;
-    p += arr;
+    L.off_rn = L.off_gx = L.off_gy = p;
+    if (stage) {
+        L.off_rn = p;
+        p += arr;
+        L.off_gx = p;
+        p += arr;
+        L.off_gy = p;
+        p += arr;
+    }
     L.bytes = (p + 127) & ~127;
     return L;
 }
 
-template <bool SIX, class Mask = uint64_t>
+template <bool SIX, class Mask = uint64_t, bool STAGE = true>
 struct WarpSolver {
     // this warp's shared memory
     uint64_t* bar;
@@ -840,6 +847,27 @@ struct WarpSolver {
         }
     }
 
+    // The reference subset at pixel i (row, col): from the staged copy, or
+    // (STAGE false) from the planes, normalised the same way.
+    __device__ __forceinline__ float rn_at(int i, int row, int col) const {
+        if constexpr (STAGE)
+            return srn[i];
+        else
+            return (__ldg(refI + ref_base + row * ref_pitch + col) - mref) * iref;
+    }
+    __device__ __forceinline__ float gx_at(int i, int row, int col) const {
+        if constexpr (STAGE)
+            return sgx[i];
+        else
+            return __ldg(refGx + ref_base + row * ref_pitch + col);
+    }
+    __device__ __forceinline__ float gy_at(int i, int row, int col) const {
+        if constexpr (STAGE)
+            return sgy[i];
+        else
+            return __ldg(refGy + ref_base + row * ref_pitch + col);
+    }
+
     // Per task: the step matrix from the pool, the reference subset staged
     // and normalised, the Ghost Wall flags and count.
     __device__ __forceinline__ void begin(const dic_task& T, float2 ms, const double* Hs21) {
@@ -866,14 +894,15 @@ struct WarpSolver {
             if (i < n) {
                 const int idx = ref_base + row * ref_pitch + col;
                 const float I = __ldg(refI + idx);
-                const float gx = __ldg(refGx + idx), gy = __ldg(refGy + idx);
                 if (I < kGhost)
                     ++g;
                 else
                     refok |= Mask(1) << k;
-                srn[i] = (I - mref) * iref;
-                sgx[i] = gx;
-                sgy[i] = gy;
+                if constexpr (STAGE) {
+                    srn[i] = (I - mref) * iref;
+                    sgx[i] = __ldg(refGx + idx);
+                    sgy[i] = __ldg(refGy + idx);
+                }
             }
             advance(row, col);
         }
@@ -1011,7 +1040,7 @@ struct WarpSolver {
         for (int k = 0; k < K; ++k) {
             if ((valid >> k) & 1u) {
                 const int i = lane + 32 * k;
-                const float g0 = sgx[i] * iref, g1 = sgy[i] * iref;
+                const float g0 = gx_at(i, row, col) * iref, g1 = gy_at(i, row, col) * iref;
                 const float fx = (float)(col - half), fy = (float)(row - half);
                 const double s[6] = {(double)g0, (double)g1, (double)(g0 * fx), (double)(g0 * fy),
                                      (double)(g1 * fx), (double)(g1 * fy)};
@@ -1080,7 +1109,8 @@ struct WarpSolver {
                 for (int k = 0; k < K; ++k) {
                     if ((valid >> k) & 1u) {
                         const int i = lane + 32 * k;
-                        const float rn = srn[i], g0 = sgx[i] * iref, g1 = sgy[i] * iref;
+                        const float rn = rn_at(i, row, col), g0 = gx_at(i, row, col) * iref,
+                                    g1 = gy_at(i, row, col) * iref;
                         const float fx = (float)(col - half), fy = (float)(row - half);
                         const float nd = (vals[i] - mean) * inv;
                         const float diff = rn - nd;
@@ -1148,14 +1178,16 @@ struct WarpSolver {
             if (sqrtf(nn) < 0.001f) {
                 // texture check on the raw reference gradients (optimization_engine.cpp:435-461)
                 float sx = 0.0f, sy = 0.0f;
+                int row = row0, col = col0;
 #pragma unroll 4
                 for (int k = 0; k < K; ++k) {
                     if ((valid >> k) & 1u) {
                         const int i = lane + 32 * k;
-                        const float gx = sgx[i], gy = sgy[i];
+                        const float gx = gx_at(i, row, col), gy = gy_at(i, row, col);
                         sx = __fmaf_rn(gx, gx, sx);
                         sy = __fmaf_rn(gy, gy, sy);
                     }
+                    advance(row, col);
                 }
                 const float tx = wsum(sx), ty = wsum(sy);
                 const float sg = ty < tx ? ty : tx;
@@ -1178,14 +1210,16 @@ struct WarpSolver {
         const bool full = cnt == n;
         const float inv = 1.0f / sdev;
         float ep = 0.0f;
+        int row = row0, col = col0;
 #pragma unroll 4
         for (int k = 0; k < K; ++k) {
             if ((valid >> k) & 1u) {
                 const int i = lane + 32 * k;
-                const float rn = srn[i];
+                const float rn = rn_at(i, row, col);
                 const float diff = full ? rn - (vals[i] - mean) * inv : rn - (vals[i] - mean) / sdev;
                 ep = __fmaf_rn(diff, diff, ep);
             }
+            advance(row, col);
         }
         const float score = wsum(ep) / (float)cnt;
         return finite_f(score) ? score : 2.0f;
@@ -1368,8 +1402,8 @@ struct WarpSolver {
 
 // Set a warp's solver up for a launch: shared-memory arrays, launch
 // constants (copied out of the by-value argument block), tile state, barrier.
-template <bool SIX, class Mask>
-__device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask>& s, unsigned char* smem, const StagedLayout& L,
+template <bool SIX, class Mask, bool STAGE>
+__device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE>& s, unsigned char* smem, const StagedLayout& L,
                                              const CUtensorMap* tmap, const float* refI, const float* refGx,
                                              const float* refGy, const float* defI, int* err, int n, int dim,
                                              int pitch, int tw, int th, int W, int H, int min_valid, int lm,
@@ -1421,14 +1455,14 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask>& s, unsigned 
 // DIMC > 0: the subset size, the tile box and the pixels per lane known at
 // compile time (the launch checks they match), so the per-pixel loop
 // bookkeeping folds away; 32-bit validity masks up to 32 pixels per lane.
-template <bool SIX, int DIMC>
+template <bool SIX, int DIMC, bool STAGE>
 __global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                   const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
     using Mask = std::conditional_t<(DIMC > 0 && DIMC * DIMC <= 1024), uint32_t, uint64_t>;
     constexpr int kTw = DIMC > 0 ? ((DIMC + (SIX ? 5 : 3) + 2 + 7 + 3) & ~3) : 0;
     constexpr int kTh = DIMC > 0 ? DIMC + (SIX ? 5 : 3) + 2 + 4 : 0;
-    WarpSolver<SIX, Mask> s;
+    WarpSolver<SIX, Mask, STAGE> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
                  DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
                  a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
@@ -1602,15 +1636,19 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
         int tw = 0, th = 0;
         tile_box(a.dim, SIX ? 1 : 0, tw, th);
         const bool box_ok = a.tile_w == 0 || (a.tile_w == tw && a.tile_h == th);
-        auto fast = fast_kernel<SIX, 0>;
-        if (box_ok && a.dim == 21) fast = fast_kernel<SIX, 21>;
-        if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31>;
-        if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41>;
-        e = cudaFuncSetAttribute(fast, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
+        // the fast pass reads the reference subset from the planes (through
+        // L1): without the staged copy a warp needs about half the shared
+        // memory, and twice as many warps fit an SM
+        auto fast = fast_kernel<SIX, 0, false>;
+        if (box_ok && a.dim == 21) fast = fast_kernel<SIX, 21, false>;
+        if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31, false>;
+        if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41, false>;
+        const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, false);
+        e = cudaFuncSetAttribute(fast, cudaFuncAttributeMaxDynamicSharedMemorySize, FL.bytes);
         if (e != cudaSuccess) return e;
-        e = one_wave(fast, SL.bytes, 0, a.n_tasks, blocks);
+        e = one_wave(fast, FL.bytes, 0, a.n_tasks, blocks);
         if (e != cudaSuccess) return e;
-        fast<<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
+        fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
         e = cudaFuncSetAttribute(rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
         if (e != cudaSuccess) return e;
         e = one_wave(rescue_kernel<SIX>, SL.bytes, cap, a.n_tasks, blocks);
