@@ -51,6 +51,11 @@ WORKLOADS = {
              "noise sigma 2, step 4, subset 31, strain window 31, 4x4 bicubic, fixed reference (frames 2+)"),
     "cfg4-plain": ("target settings: 4096x4096 uint8 speckle under the cfg1 field, noise sigma 2, step 8, "
                    "subset 41, strain window 41, 4x4 bicubic, fixed reference (frames 2+)"),
+    "cfg4-large": ("large deformation, lattice seeding from the device global-motion estimate: 4096x4096 uint8 "
+                   "speckle under a rotation ~U[0,180) deg about the centre, a translation up to 60 px and a "
+                   "smooth random field of 5 px amplitude (Gaussian covariance, length 300 px), noise sigma 2; "
+                   "step 8, subset 41, strain window 41, 4x4 bicubic; rect the centred 2744x2744 square that "
+                   "stays inside the deformed frame at any rotation; fixed reference (frames 2+)"),
 }
 WORKLOAD = WORKLOADS["cfg1"]
 
@@ -136,10 +141,11 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(ref, dfm, prm, fp64=False):
+def cpu_sample(ref, dfm, prm, fp64=False, model=None):
     """The CPU restatement on the central 1024 x 1024 ROI of the frame pair at
     the same settings, reference cache warm (the solve timed is the second on
-    the reference). Returns (points, seconds, attempted)."""
+    the reference), given the global model the device used (None: none).
+    Returns (points, seconds, attempted)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
 
@@ -149,9 +155,9 @@ def cpu_sample(ref, dfm, prm, fp64=False):
     p = [x0, x0, side, side, prm.step, prm.subset_size, prm.strain_window, prm.use_6x6_interpolator]
     o = oracle.Oracle(fp64)
     o.set_reference(ref)
-    o.run(dfm, p)  # frame 1: fills the grid scan + Hessian pool cache
+    o.run(dfm, p, model_h=model)  # frame 1: fills the grid scan + Hessian pool cache
     t0 = time.perf_counter()
-    rc, pts, met = o.run(dfm, p)
+    rc, pts, met = o.run(dfm, p, model_h=model)
     dt = time.perf_counter() - t0
     return rc, dt, int(met[0]), pts, p
 
@@ -223,9 +229,11 @@ def run_b200(args, rank, world, local_rank):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    cfg = 4 if args.workload == "cfg4-plain" else 1
     workload = WORKLOADS[args.workload]
-    ref, dfm, prm, warp = sb.config_pair(cfg, size=args.size, pair=rank)
+    if args.workload == "cfg4-large":
+        ref, dfm, prm, warp, _sim = sb.large_motion_pair(args.size, pair=rank)
+    else:
+        ref, dfm, prm, warp = sb.config_pair(4 if args.workload == "cfg4-plain" else 1, size=args.size, pair=rank)
     H, W = ref.shape
     grid_nodes = (prm.rect_w // prm.step) * (prm.rect_h // prm.step)
     capacity = grid_nodes * 8
@@ -296,12 +304,13 @@ def run_b200(args, rank, world, local_rank):
     fp32_peak = sms * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
     traffic = _ncu_traffic()
     clocks = clk.summary()
+    gm = eng.last_global_motion()
 
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu:
-            crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm)
+            crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm, model=gm["H"] if gm["locked"] else None)
             cpu = {"value": crc / cdt, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"central {cp[2]}x{cp[3]} ROI ({cp[2] // cp[4]}^2 grid, {catt} attempted) of the "
                              f"same pair, reference cache warm, {cdt:.2f} s"}
@@ -322,6 +331,8 @@ def run_b200(args, rank, world, local_rank):
             "first_frame_pool_ms": round(first_t["pool"], 3),
             "phases_ms": mean_phase,
             "mean_icgn_iters_per_point": float(met[8]),
+            "global_model": {"locked": gm["locked"], "rotation_deg": float(np.degrees(gm["theta"])),
+                             "scale": gm["scale"], "translation_px": [float(gm["t"][0]), float(gm["t"][1])]},
             "e2e": {"value": e2e_value, "unit": "points/s",
                     "h2d_bytes_per_step": int(W * H), "d2h_bytes_per_step": int(rc_e2e * 32)},
             "roofline": {"kernel": "icgn solve (Path A launch)", "bound": "fp32", "achieved": achieved,
@@ -409,8 +420,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--size", type=int, default=4096,
                     help="image edge (default 4096, the benchmark workload; smaller sizes are for profiling)")
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg4-plain", "cfg3"],
-                    help="cfg1 (the headline line), cfg4-plain (the target settings), cfg3 (incremental sample)")
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg4-plain", "cfg4-large", "cfg3"],
+                    help="cfg1 (the headline line), cfg4-plain (the target settings), cfg4-large (large "
+                         "deformation seeded by the global-motion estimate), cfg3 (incremental sample)")
     ap.add_argument("--interval", type=int, default=1, help="cfg3: the session's update_interval")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -40,6 +40,23 @@ SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], lo
    it. Returns 0, or -3 for a NULL handle. */
 SEMPER_C_API int semper_b200_set_global_model(semper_engine* eng, const double* h9);
 
+/* Switches the device global-motion estimate on (on != 0, the default) or
+   off. With no model set by semper_b200_set_global_model, each run estimates
+   a similarity (rotation, isotropic scale, translation) between the reference
+   and the deformed ROI by phase correlation and, when both correlation peaks
+   pass their gates, seeds the anchor lattice with it as the reference seeds
+   from its AKAZE homography (src/pipeline/full_field_anchors.cpp:204-279).
+   Returns 0, or -3 for a NULL or busy handle. */
+SEMPER_C_API int semper_b200_set_global_motion(semper_engine* eng, int on);
+
+/* The estimate of the last run: out[0] 1 when it was locked and used, else 0;
+   out[1] rotation (rad); out[2] scale; out[3..4] translation (px); out[5..6]
+   the centre of rotation (px); out[7..8] the rotation and translation
+   correlation peaks; out[9..17] the homography, reference -> deformed,
+   row-major. All zero but the identity homography when no estimate ran.
+   Returns 0, or -3 for a NULL or busy handle. */
+SEMPER_C_API int semper_b200_last_global_motion(semper_engine* eng, double out[18]);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -208,6 +208,10 @@ struct Engine::Impl {
 
     DevBuf<float> rI, rGx, rGy;      // reference planes
     DevBuf<uint8_t> dGray;           // deformed frame bytes
+    DevBuf<uint8_t> rGray;           // reference frame bytes (global motion)
+    bool ref_gray = false;           // rGray holds the current reference
+    const uint8_t* last_def = nullptr;
+    dic::GlobalMotion gm;
     DevBuf<float> dI, dGx, dGy;      // deformed planes (gradients kept for adoption)
     DevBuf<uint8_t> dMask;
 
@@ -479,6 +483,9 @@ void Engine::reset() {
     has_ref_ = false;
     W_ = H_ = 0;
     impl_->grid_valid = false;
+    impl_->ref_gray = false;
+    impl_->last_def = nullptr;
+    last_global_ = dic::GlobalSimilarity();
 }
 
 int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask) {
@@ -502,6 +509,9 @@ int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask
     check(dic::launch_image_prep(I.dGray.p, dm, w, h, (w + 3) & ~3, I.rI.p, I.rGx.p, I.rGy.p, stream_),
           "reference prep");
     check(cudaStreamSynchronize(stream_), "reference sync");
+    std::swap(I.rGray.p, I.dGray.p);  // the reference bytes stay for the global motion estimate
+    std::swap(I.rGray.n, I.dGray.n);
+    I.ref_gray = true;
     W_ = w;
     H_ = h;
     has_ref_ = true;
@@ -518,6 +528,13 @@ int Engine::adopt_last_deformed(const uint8_t* mask) {
     std::swap(I.rGx.n, I.dGx.n);
     std::swap(I.rGy.p, I.dGy.p);
     std::swap(I.rGy.n, I.dGy.n);
+    // the adopted frame's bytes, when the last run's frame was the engine's own copy
+    I.ref_gray = I.last_def != nullptr && I.last_def == I.dGray.p;
+    if (I.ref_gray) {
+        std::swap(I.rGray.p, I.dGray.p);
+        std::swap(I.rGray.n, I.dGray.n);
+    }
+    I.last_def = nullptr;
     if (mask) {
         // Ghost Wall on the adopted frame: the gradients stay those of the
         // real intensities (stamp after prepare, reference_cache.cpp:95-96).
@@ -694,6 +711,8 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
     const int prc = validate_params(params, W, H);
     if (prc != 0) return prc;
     E.times_ = PhaseTimes{};
+    E.last_global_ = dic::GlobalSimilarity();
+    last_def = d_def;
     try {
         poll_cancel();
         check(cudaEventRecord(ev[0], st), "event");
@@ -761,8 +780,17 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         std::vector<uint8_t> solved = h_skip;  // host mirror of the solved flags
         const int total = total_valid;
 
-        // ---------------------------------------------------------------- anchor lattice
+        // ---------------------------------------------------------------- global model
         const auto t_seed = clk::now();
+        if (!model_H && E.global_motion_ && ref_gray) {
+            dic::GlobalSimilarity& g = E.last_global_;
+            check(gm.estimate(rGray.p, d_def, W, H, params.rect_x, params.rect_y, params.rect_w, params.rect_h, st, g),
+                  "global motion");
+            E.times_.launches += g.kernels;
+            if (g.locked) model_H = g.H;
+        }
+
+        // ---------------------------------------------------------------- anchor lattice
         HostStats st_anchor, st_a, st_b;
         float globalU = 0, globalV = 0;
         bool have_model = model_H != nullptr, model_full = false, model_rejected = false;

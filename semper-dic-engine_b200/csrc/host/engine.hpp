@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include "../kernels/dic_types.h"
+#include "../kernels/globalmotion.cuh"
 
 namespace semper_b200 {
 
@@ -149,6 +150,16 @@ public:
     void clear_cancel() { h_cancel_[0] = 0; }
     bool cancel_requested() const { return h_cancel_[0] != 0; }
 
+    // Global motion (the stand-in for the AKAZE + RANSAC model,
+    // full_field_anchors.cpp:204-279): with no model passed to run, the
+    // similarity between the reference and the deformed ROI is estimated on
+    // the device and, when both of its correlation peaks pass, seeds the
+    // anchor lattice as the reference's global model does. On by default.
+    void set_global_motion(bool on) { global_motion_ = on; }
+    bool global_motion() const { return global_motion_; }
+    // The estimate of the last run (locked false: none, or none used).
+    const dic::GlobalSimilarity& last_global() const { return last_global_; }
+
     cudaStream_t stream() const { return stream_; }
     const PhaseTimes& last_times() const { return times_; }
     // Grid blocks of the persistent solve kernel (0: automatic).
@@ -164,6 +175,8 @@ private:
     bool has_ref_ = false;
     int W_ = 0, H_ = 0;
     int solve_blocks_ = 0;
+    bool global_motion_ = true;
+    dic::GlobalSimilarity last_global_;
     PhaseTimes times_;
     friend struct Impl;
 };

@@ -110,7 +110,10 @@ struct IncrementalSession::Impl {
     semper_inc::IncrementalCore<DeviceBackend> core{backend};
 };
 
-IncrementalSession::IncrementalSession() : impl_(new Impl()) {}
+// The session solves without a global model: the motion between a frame and
+// its (updated) reference stays small, and the restatement the session is
+// checked against runs the same way.
+IncrementalSession::IncrementalSession() : impl_(new Impl()) { impl_->engine.set_global_motion(false); }
 IncrementalSession::~IncrementalSession() = default;
 
 void IncrementalSession::reset() {

@@ -238,6 +238,32 @@ SEMPER_C_API int semper_b200_set_global_model(semper_engine* eng, const double* 
     return 0;
 }
 
+SEMPER_C_API int semper_b200_set_global_motion(semper_engine* eng, int on) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    eng->engine.set_global_motion(on != 0);
+    return 0;
+}
+
+SEMPER_C_API int semper_b200_last_global_motion(semper_engine* eng, double out[18]) {
+    if (eng == nullptr || out == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    const dic::GlobalSimilarity& g = eng->engine.last_global();
+    out[0] = g.locked ? 1.0 : 0.0;
+    out[1] = g.theta;
+    out[2] = g.scale;
+    out[3] = g.tx;
+    out[4] = g.ty;
+    out[5] = g.cx;
+    out[6] = g.cy;
+    out[7] = g.peak_rotation;
+    out[8] = g.peak_translation;
+    for (int i = 0; i < 9; ++i) out[9 + i] = g.H[i];
+    return 0;
+}
+
 SEMPER_C_API semper_incremental* semper_incremental_create(void) {
     return guarded<semper_incremental*>(nullptr, [] {
         auto* inc = new semper_incremental();

@@ -36,7 +36,7 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
              "semper_incremental_create", "semper_incremental_destroy", "semper_incremental_init",
              "semper_incremental_process", "semper_run", "semper_set_reference", "semper_version"]
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
-               "semper_b200_stream"]
+               "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -94,6 +94,8 @@ def lib():
         L.semper_b200_stream.restype = _vp
         L.semper_b200_last_timings.argtypes = [_vp, _f32p, ctypes.POINTER(ctypes.c_longlong)]
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
+        L.semper_b200_set_global_motion.argtypes = [_vp, ctypes.c_int]
+        L.semper_b200_last_global_motion.argtypes = [_vp, _f64p]
         L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 3 + [_vp] * 4
         L.dic_cuda_grid_scan.argtypes = [_vp] + [ctypes.c_int] * 8 + [_vp, _vp, _vp]
         L.dic_cuda_hessian_pool.argtypes = [_vp] * 3 + [ctypes.c_int] * 3 + [_vp] + [ctypes.c_int] * 7 + [_vp] * 5
@@ -197,6 +199,16 @@ class Engine:
         Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
         return lib().semper_b200_set_global_model(self._h, _p(Hm, _f64p))
 
+    def set_global_motion(self, on: bool) -> int:
+        return lib().semper_b200_set_global_motion(self._h, 1 if on else 0)
+
+    def last_global_motion(self) -> dict:
+        """The similarity the last run estimated (semper_b200_last_global_motion)."""
+        o = np.zeros(18, np.float64)
+        lib().semper_b200_last_global_motion(self._h, _p(o, _f64p))
+        return {"locked": bool(o[0]), "theta": o[1], "scale": o[2], "t": (o[3], o[4]), "centre": (o[5], o[6]),
+                "peaks": (o[7], o[8]), "H": o[9:].reshape(3, 3).copy()}
+
 
 class Incremental:
     """semper_incremental: a frame sequence against a moving reference."""
@@ -297,6 +309,51 @@ def config_pair(cfg: int, size: int | None = None, pair: int = 0):
     ref = speckle(n, n, 1000 + pair)
     dfm = speckle(n, n, 1000 + pair, warp, noise, 2000 + 1)
     return ref, dfm, prm, warp
+
+
+def large_motion_pair(size: int | None = None, pair: int = 0, angle_deg: float | None = None,
+                      shift: tuple | None = None, grf_px: float = 5.0, grf_len: float = 300.0, modes: int = 16):
+    """(reference, deformed, params, warp, similarity) of the large-deformation
+    workload: 4096^2 speckle under a rigid rotation ~ U[0, 180) deg about the
+    image centre and a translation of up to 60 px, plus a smooth random
+    displacement field of amplitude `grf_px` (per component a sum of `modes`
+    cosines with wavevectors ~ N(0, grf_len^-2) per axis, a Gaussian
+    covariance of length grf_len, and random phases, scaled so that the
+    field's largest magnitude over the frame, sampled every 16 px, is
+    grf_px), noise sigma 2; step 8, subset 41, window 41.
+    The rect is the centred square whose every subset stays inside the
+    deformed frame at any rotation (side (n/2 - 105) sqrt 2, rounded down to
+    the step: 105 px cover the 60 px translation, the random field, half a
+    subset and the interpolation border), so that the anchor lattice can keep
+    a global model (at least 90% of its anchors solved).
+    `similarity` = (angle rad, tx, ty) of the rigid part."""
+    n = size or 4096
+    rng = np.random.default_rng(7000 + pair)
+    th = np.radians(rng.uniform(0.0, 180.0) if angle_deg is None else angle_deg)
+    if shift is None:
+        r, phi = 60.0 * np.sqrt(rng.uniform()), rng.uniform(0.0, 2 * np.pi)
+        shift = (r * np.cos(phi), r * np.sin(phi))
+    a = (np.cos(th) - 1.0, -np.sin(th), np.sin(th), np.cos(th) - 1.0)
+    md = []
+    if grf_px != 0.0:
+        for c in range(2 * modes):
+            k = rng.normal(0.0, 1.0 / grf_len, 2)
+            md.append([k[0], k[1], 1.0 if c % 2 == 0 else 0.0, 1.0 if c % 2 == 1 else 0.0,
+                       rng.uniform(0.0, 2 * np.pi)])
+        g = np.arange(0.0, n, 16.0)
+        X, Y = np.meshgrid(g, g)
+        u, v = displacement(warp_block(modes=md), X, Y)
+        scale = grf_px / float(np.max(np.hypot(u, v)))
+        for m in md:
+            m[2] *= scale
+            m[3] *= scale
+    warp = warp_block(cx=n / 2, cy=n / 2, u0=shift[0], v0=shift[1], a=a, modes=[tuple(m) for m in md])
+    side = int((n / 2 - 105) * np.sqrt(2.0)) // 8 * 8
+    x0 = (n - side) // 2
+    prm = params((x0, x0, side, side), 8, 41, 41)
+    ref = speckle(n, n, 4000 + pair)
+    dfm = speckle(n, n, 4000 + pair, warp, 2.0, 5000 + pair)
+    return ref, dfm, prm, warp, (float(th), float(shift[0]), float(shift[1]))
 
 
 # --------------------------------------------------------------- kernel-level stages (torch device tensors)

@@ -168,14 +168,18 @@ def test_median_vsg_bit_exact():
 
 
 def _run_both(ref, dfm, prm, mask=None, capacity=None):
+    """The device engine (global motion on, its default) and the restatement
+    given the model the device estimated, as the reference's golden scenarios
+    inject their AKAZE model."""
     e = sb.Engine()
     assert e.set_reference(ref, mask) == 0
     rc, pts, met = e.run(dfm, prm, capacity=capacity, mask=mask)
+    g = e.last_global_motion()
     o = oracle.Oracle(False)
     o.set_reference(ref, mask)
     p = [prm.rect_x, prm.rect_y, prm.rect_w, prm.rect_h, prm.step, prm.subset_size, prm.strain_window,
          prm.use_6x6_interpolator]
-    orc, opts, omet = o.run(dfm, p, capacity=capacity, mask=mask)
+    orc, opts, omet = o.run(dfm, p, capacity=capacity, mask=mask, model_h=g["H"] if g["locked"] else None)
     return (rc, pts, met), (orc, opts, omet)
 
 
