@@ -57,6 +57,38 @@ SEMPER_C_API int semper_b200_set_global_motion(semper_engine* eng, int on);
    Returns 0, or -3 for a NULL or busy handle. */
 SEMPER_C_API int semper_b200_last_global_motion(semper_engine* eng, double out[18]);
 
+/* Batched solves: many independent pairs, each with its own size, mask and
+   settings, solved concurrently on the current device. No counterpart in the
+   reference (its callers loop over semper_set_reference + semper_run); each
+   job's result, metrics and return code are exactly those of that loop on a
+   fresh handle. */
+typedef struct semper_b200_job {
+    const uint8_t* reference; /* width*height gray bytes */
+    const uint8_t* deformed;  /* width*height gray bytes */
+    const uint8_t* mask;      /* width*height bytes (>= 128: material), or NULL */
+    int32_t width, height;
+    semper_params params;
+    float* out;               /* out_capacity floats: packed points, as semper_run */
+    int32_t out_capacity;
+    float* metrics;           /* metrics_len floats, or NULL */
+    int32_t metrics_len;
+    int32_t result;           /* written: semper_run's return value for this job */
+} semper_b200_job;
+
+typedef struct semper_b200_batch semper_b200_batch;
+
+/* A batch runner with `workers` engines (<= 0: 4), each with its own stream
+   and host thread, on the current device. NULL on failure. */
+SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers);
+SEMPER_C_API void semper_b200_batch_destroy(semper_b200_batch* b);
+/* Solves every job (largest first, spread over the workers) and returns 0
+   when all have run (each job's own code is in its `result`), or -3 for a
+   NULL or busy runner. Job buffers must stay valid until it returns. */
+SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jobs, int32_t n_jobs);
+/* The first internal failure (a CUDA error) of the last batch_run, "" when
+   none; valid until the next call on the runner. */
+SEMPER_C_API const char* semper_b200_batch_last_error(semper_b200_batch* b);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

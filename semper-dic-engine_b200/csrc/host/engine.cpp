@@ -649,7 +649,7 @@ PatchSolve Engine::solve_patch(const uint8_t* patch, int size, int ax, int ay, f
     I.launched(1, dic::launch_image_prep(I.aGray.p, nullptr, size, size, pp, I.aI.p, I.aGx.p, I.aGy.p, st),
                "patch prep");
     check(cudaMemsetAsync(I.aSkip.p, 0, 1, st), "memset");
-    I.launched(1, dic::launch_pool(I.aI.p, I.aGx.p, I.aGy.p, size, size, pp, I.aSkip.p, 1, 1, c, c, 1, subset, 1,
+    I.launched(2, dic::launch_pool(I.aI.p, I.aGx.p, I.aGy.p, size, size, pp, I.aSkip.p, 1, 1, c, c, 1, subset, 1,
                                    I.aValid.p, reinterpret_cast<float2*>(I.aMs.p), nullptr, I.aHs.p, st),
                "patch pool");
     dic_task t{};
@@ -750,7 +750,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             pool_valid.ensure(NG);
             pool_ms.ensure(NG);
             pool_Hs.ensure(NG * 21);
-            launched(1, dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, pitch(), skip.p, gW, gH, params.rect_x, params.rect_y,
+            launched(2, dic::launch_pool(rI.p, rGx.p, rGy.p, W, H, pitch(), skip.p, gW, gH, params.rect_x, params.rect_y,
                                    params.step, dim, 1, pool_valid.p, pool_ms.p, nullptr, pool_Hs.p, st),
                   "pool");
             h_skip.resize(NG);

@@ -1103,17 +1103,28 @@ struct WarpSolver {
             const float inv = 1.0f / sdev;
 
             float ep = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f, gp3 = 0.0f, gp4 = 0.0f, gp5 = 0.0f;
-            {
+            // one pixel's share of the residual and the steepest-descent sums
+            auto accumulate = [&](int i, float I, float gx, float gy, float fx, float fy) {
+                const float rn = (I - mref) * iref, g0 = gx * iref, g1 = gy * iref;
+                const float nd = (vals[i] - mean) * inv;
+                const float diff = rn - nd;
+                ep = __fmaf_rn(diff, diff, ep);
+                gp0 = __fmaf_rn(g0, diff, gp0);
+                gp1 = __fmaf_rn(g1, diff, gp1);
+                gp2 = __fmaf_rn(g0 * fx, diff, gp2);
+                gp3 = __fmaf_rn(g0 * fy, diff, gp3);
+                gp4 = __fmaf_rn(g1 * fx, diff, gp4);
+                gp5 = __fmaf_rn(g1 * fy, diff, gp5);
+            };
+            if constexpr (STAGE) {
                 int row = row0, col = col0;
 #pragma unroll 4
                 for (int k = 0; k < K; ++k) {
                     if ((valid >> k) & 1u) {
                         const int i = lane + 32 * k;
-                        const float rn = rn_at(i, row, col), g0 = gx_at(i, row, col) * iref,
-                                    g1 = gy_at(i, row, col) * iref;
+                        const float diff = srn[i] - (vals[i] - mean) * inv;
+                        const float g0 = sgx[i] * iref, g1 = sgy[i] * iref;
                         const float fx = (float)(col - half), fy = (float)(row - half);
-                        const float nd = (vals[i] - mean) * inv;
-                        const float diff = rn - nd;
                         ep = __fmaf_rn(diff, diff, ep);
                         gp0 = __fmaf_rn(g0, diff, gp0);
                         gp1 = __fmaf_rn(g1, diff, gp1);
@@ -1123,6 +1134,47 @@ struct WarpSolver {
                         gp5 = __fmaf_rn(g1 * fy, diff, gp5);
                     }
                     advance(row, col);
+                }
+            } else {
+                // The reference comes from the planes (L2): the loads of the
+                // next four pixels are issued before the current four are
+                // summed, so their latency overlaps the arithmetic.
+                constexpr int G = 4;
+                float nI[G], nX[G], nY[G], nfx[G], nfy[G];
+                int lr = row0, lc = col0;
+                auto fetch = [&](int k0) {
+#pragma unroll
+                    for (int u = 0; u < G; ++u) {
+                        const int k = k0 + u;
+                        nI[u] = nX[u] = nY[u] = 0.0f;
+                        nfx[u] = (float)(lc - half);
+                        nfy[u] = (float)(lr - half);
+                        if (k < K && lane + 32 * k < n) {
+                            const int idx = ref_base + lr * ref_pitch + lc;
+                            nI[u] = __ldg(refI + idx);
+                            nX[u] = __ldg(refGx + idx);
+                            nY[u] = __ldg(refGy + idx);
+                        }
+                        advance(lr, lc);
+                    }
+                };
+                fetch(0);
+                for (int k0 = 0; k0 < K; k0 += G) {
+                    float cI[G], cX[G], cY[G], cfx[G], cfy[G];
+#pragma unroll
+                    for (int u = 0; u < G; ++u) {
+                        cI[u] = nI[u];
+                        cX[u] = nX[u];
+                        cY[u] = nY[u];
+                        cfx[u] = nfx[u];
+                        cfy[u] = nfy[u];
+                    }
+                    if (k0 + G < K) fetch(k0 + G);
+#pragma unroll
+                    for (int u = 0; u < G; ++u) {
+                        const int k = k0 + u;
+                        if (k < K && ((valid >> k) & 1u)) accumulate(lane + 32 * k, cI[u], cX[u], cY[u], cfx[u], cfy[u]);
+                    }
                 }
             }
             const float err2 = wsum(ep);
@@ -1456,7 +1508,7 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE>& s, un
 // compile time (the launch checks they match), so the per-pixel loop
 // bookkeeping folds away; 32-bit validity masks up to 32 pixels per lane.
 template <bool SIX, int DIMC, bool STAGE>
-__global__ void __launch_bounds__(32) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
+__global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                   const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
     using Mask = std::conditional_t<(DIMC > 0 && DIMC * DIMC <= 1024), uint32_t, uint64_t>;
@@ -1664,17 +1716,17 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
     return cudaGetLastError();
 }
 
+// The driver's tensor-map encoder, looked up once per process (a function
+// static: thread-safe initialisation, engines may run on several threads).
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+    }();
     return fn;
 }
 

@@ -87,13 +87,15 @@ __global__ void scan_kernel(const uint8_t* __restrict__ mask, int W, int H, int 
 }
 
 // One warp per node of the pool: mean and std over non-Ghost pixels (FP32,
-// lane partial sums + butterfly), the 21-entry Gauss-Newton Hessian (FP64),
-// then the 2x2 and scaled-rcond checks on lane 0.
-__global__ void pool_kernel(const float* __restrict__ I, const float* __restrict__ Gx,
-                            const float* __restrict__ Gy, int W, int H, int pitch, const uint8_t* __restrict__ skip,
-                            int gridW, int gridH, int rect_x, int rect_y, int step, int dim, int lm,
-                            uint8_t* __restrict__ valid, float2* __restrict__ ms, double* __restrict__ H21,
-                            double* __restrict__ Hs21) {
+// lane partial sums + butterfly) and the 21-entry Gauss-Newton Hessian
+// (FP64), written to Hs21 for pool_finish_kernel. A node that is skipped,
+// off the image or less than half valid is marked invalid here (flag 0) and
+// left alone by the finish; the others get flag 2 ("sums ready").
+__global__ void pool_sums_kernel(const float* __restrict__ I, const float* __restrict__ Gx,
+                                 const float* __restrict__ Gy, int W, int H, int pitch,
+                                 const uint8_t* __restrict__ skip, int gridW, int gridH, int rect_x, int rect_y,
+                                 int step, int dim, uint8_t* __restrict__ valid, float2* __restrict__ ms,
+                                 double* __restrict__ Hs21) {
     const int node = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (node >= gridW * gridH) return;
@@ -101,15 +103,15 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     const int cx = rect_x + (node % gridW) * step, cy = rect_y + (node / gridW) * step;
     const bool ok_dim = dim >= 3 && (dim & 1);
     const bool on = cx - half >= 0 && cx + half < W && cy - half >= 0 && cy + half < H;
-    if ((skip && skip[node]) || !ok_dim || !on) {
+    auto invalid = [&]() {
         if (lane == 0) {
             valid[node] = 0;
             ms[node] = make_float2(0.0f, 1.0f);
         }
-        if (lane < 21) {
-            if (H21) H21[(size_t)node * 21 + lane] = 0.0;
-            Hs21[(size_t)node * 21 + lane] = 0.0;
-        }
+        if (lane < 21) Hs21[(size_t)node * 21 + lane] = 0.0;
+    };
+    if ((skip && skip[node]) || !ok_dim || !on) {
+        invalid();
         return;
     }
     const size_t base = (size_t)(cy - half) * pitch + (cx - half);
@@ -132,14 +134,7 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     cnt = wsum(cnt);
     const float sum = wsum(part);
     if ((float)cnt < (float)n * 0.5f) {
-        if (lane == 0) {
-            valid[node] = 0;
-            ms[node] = make_float2(0.0f, 1.0f);
-        }
-        if (lane < 21) {
-            if (H21) H21[(size_t)node * 21 + lane] = 0.0;
-            Hs21[(size_t)node * 21 + lane] = 0.0;
-        }
+        invalid();
         return;
     }
     const float mean = sum / (float)cnt;
@@ -184,40 +179,53 @@ __global__ void pool_kernel(const float* __restrict__ I, const float* __restrict
     }
 #pragma unroll
     for (int k = 0; k < 21; ++k) hp[k] = wsum(hp[k]);
-    if (H21 && lane < 21) {
+    if (lane < 21) {
         double v = 0.0;
 #pragma unroll
         for (int k = 0; k < 21; ++k)
             if (k == lane) v = hp[k];
-        H21[(size_t)node * 21 + lane] = v;
+        Hs21[(size_t)node * 21 + lane] = v;
     }
     if (lane == 0) {
-        double Hm[6][6], Hs[6][6];
-        for (int a = 0; a < 6; ++a)
-            for (int b = a; b < 6; ++b) {
-                Hm[a][b] = hp[tri21(a, b)];
-                Hm[b][a] = Hm[a][b];
-            }
-        const bool good = cond2x2_ok(Hm) && well_conditioned(Hm, half);
-        valid[node] = good ? 1 : 0;
+        valid[node] = 2;
         ms[node] = make_float2(mean, sd);
-        // The step matrix of a whole-subset iteration (optimization_engine.cpp:
-        // 302-315): the LM-damped inverse when damping is on and the damped
-        // matrix is well conditioned, else the plain inverse.
-        bool done = false;
-        if (good && lm) {
-            double Hd[6][6];
-            for (int a = 0; a < 6; ++a)
-                for (int b = 0; b < 6; ++b) Hd[a][b] = Hm[a][b];
-            Hd[0][0] += (double)0.05f;
-            Hd[1][1] += (double)0.05f;
-            if (well_conditioned(Hd, half) && inverse6(Hd, Hs)) done = true;
-        }
-        if (good && !done && !inverse6(Hm, Hs)) valid[node] = 0;
-        double* o = Hs21 + (size_t)node * 21;
-        for (int a = 0; a < 6; ++a)
-            for (int b = a; b < 6; ++b) o[tri21(a, b)] = good ? Hs[a][b] : 0.0;
     }
+}
+
+// One thread per node whose sums are ready: the 2x2 and scaled-rcond checks
+// and the step matrix of a whole-subset iteration (optimization_engine.cpp:
+// 302-315): the LM-damped inverse when damping is on and the damped matrix is
+// well conditioned, else the plain inverse. Hs21 holds the Hessian on entry
+// (copied to H21 when given) and the step matrix on return. The 6x6 FP64 work
+// is serial per node, so nodes run one per thread rather than one per warp.
+__global__ void pool_finish_kernel(int nodes, int half, int lm, uint8_t* __restrict__ valid,
+                                   double* __restrict__ H21, double* __restrict__ Hs21) {
+    const int node = blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= nodes || valid[node] != 2) return;
+    double* o = Hs21 + (size_t)node * 21;
+    double Hm[6][6], Hs[6][6];
+    for (int a = 0; a < 6; ++a)
+        for (int b = a; b < 6; ++b) {
+            Hm[a][b] = o[tri21(a, b)];
+            Hm[b][a] = Hm[a][b];
+        }
+    if (H21)
+        for (int k = 0; k < 21; ++k) H21[(size_t)node * 21 + k] = o[k];
+    const bool good = cond2x2_ok(Hm) && well_conditioned(Hm, half);
+    uint8_t v = good ? 1 : 0;
+    bool done = false;
+    if (good && lm) {
+        double Hd[6][6];
+        for (int a = 0; a < 6; ++a)
+            for (int b = 0; b < 6; ++b) Hd[a][b] = Hm[a][b];
+        Hd[0][0] += (double)0.05f;
+        Hd[1][1] += (double)0.05f;
+        if (well_conditioned(Hd, half) && inverse6(Hd, Hs)) done = true;
+    }
+    if (good && !done && !inverse6(Hm, Hs)) v = 0;
+    for (int a = 0; a < 6; ++a)
+        for (int b = a; b < 6; ++b) o[tri21(a, b)] = good ? Hs[a][b] : 0.0;
+    valid[node] = v;
 }
 
 }  // namespace
@@ -245,8 +253,13 @@ cudaError_t launch_pool(const float* I, const float* gx, const float* gy, int W,
                         float2* ms, double* H21, double* Hs21, cudaStream_t st) {
     const int nodes = gridW * gridH;
     const int wpb = 4;
-    pool_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(I, gx, gy, W, H, pitch, skip, gridW, gridH, rect_x,
-                                                               rect_y, step, dim, lm, valid, ms, H21, Hs21);
+    pool_sums_kernel<<<(nodes + wpb - 1) / wpb, wpb * 32, 0, st>>>(I, gx, gy, W, H, pitch, skip, gridW, gridH,
+                                                                    rect_x, rect_y, step, dim, valid, ms, Hs21);
+    if (H21) {
+        const cudaError_t e = cudaMemsetAsync(H21, 0, (size_t)nodes * 21 * sizeof(double), st);
+        if (e != cudaSuccess) return e;
+    }
+    pool_finish_kernel<<<(nodes + 127) / 128, 128, 0, st>>>(nodes, dim / 2, lm, valid, H21, Hs21);
     return cudaGetLastError();
 }
 

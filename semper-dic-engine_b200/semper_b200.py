@@ -36,7 +36,9 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
              "semper_incremental_create", "semper_incremental_destroy", "semper_incremental_init",
              "semper_incremental_process", "semper_run", "semper_set_reference", "semper_version"]
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
-               "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion"]
+               "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion",
+               "semper_b200_batch_create", "semper_b200_batch_destroy", "semper_b200_batch_run",
+               "semper_b200_batch_last_error"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -53,6 +55,14 @@ class IncrementalInfo(ctypes.Structure):
     _fields_ = [("reference_frame", ctypes.c_int32), ("reference_updated", ctypes.c_int32),
                 ("tracked_points", ctypes.c_int32), ("frame0_points", ctypes.c_int32),
                 ("taylor_fallbacks", ctypes.c_int32), ("lost_this_frame", ctypes.c_int32)]
+
+
+class BatchJob(ctypes.Structure):
+    """semper_b200_job (include/semper_b200_ext.h)."""
+    _fields_ = [("reference", ctypes.c_void_p), ("deformed", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("params", SemperParams),
+                ("out", ctypes.c_void_p), ("out_capacity", ctypes.c_int32), ("metrics", ctypes.c_void_p),
+                ("metrics_len", ctypes.c_int32), ("result", ctypes.c_int32)]
 
 
 PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_void_p)
@@ -95,6 +105,12 @@ def lib():
         L.semper_b200_last_timings.argtypes = [_vp, _f32p, ctypes.POINTER(ctypes.c_longlong)]
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
         L.semper_b200_set_global_motion.argtypes = [_vp, ctypes.c_int]
+        L.semper_b200_batch_create.argtypes = [ctypes.c_int32]
+        L.semper_b200_batch_create.restype = _vp
+        L.semper_b200_batch_destroy.argtypes = [_vp]
+        L.semper_b200_batch_run.argtypes = [_vp, ctypes.POINTER(BatchJob), ctypes.c_int32]
+        L.semper_b200_batch_last_error.argtypes = [_vp]
+        L.semper_b200_batch_last_error.restype = ctypes.c_char_p
         L.semper_b200_last_global_motion.argtypes = [_vp, _f64p]
         L.dic_cuda_image_prep.argtypes = [_vp] * 2 + [ctypes.c_int] * 3 + [_vp] * 4
         L.dic_cuda_grid_scan.argtypes = [_vp] + [ctypes.c_int] * 8 + [_vp, _vp, _vp]
@@ -208,6 +224,98 @@ class Engine:
         lib().semper_b200_last_global_motion(self._h, _p(o, _f64p))
         return {"locked": bool(o[0]), "theta": o[1], "scale": o[2], "t": (o[3], o[4]), "centre": (o[5], o[6]),
                 "peaks": (o[7], o[8]), "H": o[9:].reshape(3, 3).copy()}
+
+
+class Batch:
+    """semper_b200_batch: independent pairs solved concurrently."""
+
+    def __init__(self, workers: int = 4):
+        self._h = lib().semper_b200_batch_create(workers)
+        if not self._h:
+            raise RuntimeError("semper_b200_batch_create failed")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().semper_b200_batch_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def run(self, jobs, metrics_len: int = 24):
+        """jobs: dicts with ref, dfm, prm and optionally mask and capacity.
+        Returns one (rc, points, metrics) per job, in the jobs' order."""
+        keep, arr = [], (BatchJob * max(len(jobs), 1))()
+        outs = []
+        for k, j in enumerate(jobs):
+            ref = np.ascontiguousarray(j["ref"], np.uint8)
+            dfm = np.ascontiguousarray(j["dfm"], np.uint8)
+            m = j.get("mask")
+            m = None if m is None else np.ascontiguousarray(m, np.uint8)
+            prm = j["prm"]
+            cap = j.get("capacity")
+            if cap is None:
+                cap = max(prm.rect_w // max(prm.step, 1), 1) * max(prm.rect_h // max(prm.step, 1), 1) * 8
+            out = np.zeros(max(cap, 1), np.float32)
+            met = np.zeros(max(metrics_len, 1), np.float32)
+            keep += [ref, dfm, m, out, met]
+            outs.append((out, met))
+            b = arr[k]
+            b.reference, b.deformed = ref.ctypes.data, dfm.ctypes.data
+            b.mask = None if m is None else m.ctypes.data
+            b.height, b.width = ref.shape
+            b.params = prm
+            b.out, b.out_capacity = out.ctypes.data, cap
+            b.metrics, b.metrics_len = met.ctypes.data, metrics_len
+            b.result = 0
+        rc = lib().semper_b200_batch_run(self._h, arr, len(jobs))
+        if rc != 0:
+            raise RuntimeError(f"semper_b200_batch_run returned {rc}")
+        self.last_error = (lib().semper_b200_batch_last_error(self._h) or b"").decode()
+        res = []
+        for k, (out, met) in enumerate(outs):
+            r = arr[k].result
+            res.append((r, out[: max(r, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy()))
+        return res
+
+
+def batch_jobs(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int = 2048):
+    """The batched uneven workload: n independent pairs, side ~ U{min_side..
+    max_side} (square frames of seeded speckle as cfg0), each under its own
+    affine warp (|rotation| <= 10 deg, stretch <= 3 % per axis, translation
+    <= 8 px, about the frame centre) with noise sigma 1, and its own random
+    circular holes in the mask (1-3 discs removing a fraction ~ U[0, 0.4] of
+    the frame); per pair subset ~ {15, 21, 31, 41}, step ~ {4, 8},
+    strain window = subset, the whole frame as ROI."""
+    rng = np.random.default_rng(9000 + seed)
+    jobs = []
+    for k in range(n):
+        side = int(rng.integers(min_side, max_side + 1))
+        th = np.radians(rng.uniform(-10.0, 10.0))
+        sx, sy = 1.0 + rng.uniform(-0.03, 0.03), 1.0 + rng.uniform(-0.03, 0.03)
+        c, s_ = np.cos(th), np.sin(th)
+        a = (c * sx - 1.0, -s_ * sy, s_ * sx, c * sy - 1.0)
+        t = rng.uniform(-8.0, 8.0, 2)
+        warp = warp_block(cx=side / 2, cy=side / 2, u0=t[0], v0=t[1], a=a)
+        frac = rng.uniform(0.0, 0.4)
+        nd = int(rng.integers(1, 4))
+        mask = None
+        if frac > 0.0:
+            mask = np.full((side, side), 255, np.uint8)
+            r = side * np.sqrt(frac / (nd * np.pi))
+            for _ in range(nd):
+                cx_, cy_ = rng.uniform(0, side, 2)
+                x0, x1 = max(int(cx_ - r), 0), min(int(cx_ + r) + 2, side)
+                y0, y1 = max(int(cy_ - r), 0), min(int(cy_ + r) + 2, side)
+                yy, xx = np.mgrid[y0:y1, x0:x1]
+                sub = mask[y0:y1, x0:x1]
+                sub[(xx - cx_) ** 2 + (yy - cy_) ** 2 < r * r] = 0
+        subset = int(rng.choice([15, 21, 31, 41]))
+        step = int(rng.choice([4, 8]))
+        ref = speckle(side, side, 10000 + 17 * seed + k)
+        dfm = speckle(side, side, 10000 + 17 * seed + k, warp, 1.0, 20000 + k)
+        jobs.append({"ref": ref, "dfm": dfm, "mask": mask, "prm": params((0, 0, side, side), step, subset, subset),
+                     "warp": warp})
+    return jobs
 
 
 class Incremental:
