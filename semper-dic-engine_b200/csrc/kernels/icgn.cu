@@ -1,5 +1,11 @@
 // Batched subset solves: IC-GN with its Simplex rescue and coarse search,
-// one warp per subset, a persistent grid pulling tasks from a device queue.
+// a persistent grid pulling tasks from a device queue. Three kernels:
+// - fast_kernel: one warp per subset, the common case (whole-subset IC-GN);
+//   every other task is handed to a list;
+// - coop_rescue_kernel: the tasks on that list, with every path, a block of
+//   kCoopWarps warps per task (the sampling of each evaluation shared);
+// - solve_kernel: every task of a launch whose subsets are too large for the
+//   staged solvers (side > 45).
 //
 // Restates, per task, solve_node (src/pipeline/full_field_solver.cpp:119-139)
 // -> calculate_deformation (src/math/optimization_engine.cpp:55-118) ->
@@ -785,11 +791,23 @@ constexpr int kFastMaxSmem = 227 * 1024;
 
 struct StagedLayout {
     int off_tile, off_vals, off_rn, off_gx, off_gy;
-    int bytes;  // per warp, a multiple of 128
+    int off_coop;  // the cooperative rescue's request block and guard bits (0: none)
+    int bytes;     // per warp (per block for the cooperative rescue), a multiple of 128
 };
 
-// stage false: no staged reference subset (the solver reads the planes)
-StagedLayout staged_layout(int n, int tw, int th, bool stage = true) {
+// The cooperative rescue: warp 0 of a block drives a task, and every warp of
+// the block samples a share of the subset for each evaluation.
+constexpr int kCoopWarps = 8;
+struct CoopReq {
+    int op;  // 0: done, 1: sample, 2: coarse search
+    int cx, cy, tile_ok, tx0, ty0;
+    float Wp[6];
+};
+constexpr int kCoopBytes = 64 + kCoopWarps * 32 * 8 + kCoopWarps * 8;
+
+// stage false: no staged reference subset (the solver reads the planes);
+// coop: room for the cooperative rescue's request block
+StagedLayout staged_layout(int n, int tw, int th, bool stage = true, bool coop = false) {
     StagedLayout L;
     L.off_tile = 640;
     int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
@@ -805,11 +823,19 @@ StagedLayout staged_layout(int n, int tw, int th, bool stage = true) {
         L.off_gy = p;
         p += arr;
     }
+    L.off_coop = 0;
+    if (coop) {
+        p = (p + 127) & ~127;
+        L.off_coop = p;
+        p += kCoopBytes;
+    }
     L.bytes = (p + 127) & ~127;
     return L;
 }
 
-template <bool SIX, class Mask = uint64_t, bool STAGE = true>
+__device__ __forceinline__ void coop_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kCoopWarps * 32) : "memory"); }
+
+template <bool SIX, class Mask = uint64_t, bool STAGE = true, bool COOP = false>
 struct WarpSolver {
     // this warp's shared memory
     uint64_t* bar;
@@ -837,6 +863,12 @@ struct WarpSolver {
     int cx, cy, ref_base, ghost;
     float mref, iref, lo_x, hi_x, lo_y, hi_y;
     Mask refok;
+    // COOP: the block's request block, guard bits (kCoopWarps x 32) and
+    // coarse-search slots, and this warp's index in the block
+    CoopReq* req;
+    Mask* gbits;
+    float2* cslots;
+    int warp;
 
     __device__ __forceinline__ void advance(int& row, int& col) const {
         col += r;
@@ -965,12 +997,118 @@ struct WarpSolver {
         }
     }
 
+    // The pixels k in [k_lo, k_hi) of this lane (i = lane + 32 k): their
+    // values into vals and the guard bits (inside the 4 px guard) returned.
+    // Four pixels' loads are issued before their stores.
+    __device__ __forceinline__ Mask sample_part(const float Wp[6], int k_lo, int k_hi) {
+        Mask g = 0;
+        const int i0 = lane + 32 * k_lo;
+        int row = i0 / dim, col = i0 - (i0 / dim) * dim;
+        for (int k0 = k_lo; k0 < k_hi; k0 += 4) {
+            float v[4];
+            int ii[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int k = k0 + u;
+                ii[u] = lane + 32 * k;
+                v[u] = 0.0f;
+                if (k < k_hi && ii[u] < n) {
+                    const float ox = (float)(col - half), oy = (float)(row - half);
+                    const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
+                    const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
+                    const float rx = fx + 0.5f, ry = fy + 0.5f;
+                    if (rx >= lo_x && rx < hi_x && ry >= lo_y && ry < hi_y) {
+                        const float flx = floorf(fx), fly = floorf(fy);
+                        const int xi = cx + (int)flx, yi = cy + (int)fly;
+                        const int lx = xi - tx0, ly = yi - ty0;
+                        if (tile_ok)
+                            v[u] = SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly)
+                                       : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
+                        else
+                            v[u] = SIX ? interp6(defI, pitch, xi, yi, fx - flx, fy - fly)
+                                       : interp4(defI, pitch, xi, yi, fx - flx, fy - fly);
+                        g |= Mask(1) << k;
+                    }
+                }
+                advance(row, col);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (k0 + u < k_hi && ii[u] < n) vals[ii[u]] = v[u];
+        }
+        return g;
+    }
+
+    // COOP, warps 1..: serve the driver's requests until it is done.
+    __device__ void coop_serve() {
+        const int per = (K + kCoopWarps - 1) / kCoopWarps;
+        for (;;) {
+            coop_bar();  // a request is posted
+            const int op = req->op;
+            if (op == 0) break;
+            cx = req->cx;
+            cy = req->cy;
+            lo_x = (float)(4 - cx);
+            hi_x = (float)(W - 4 - cx);
+            lo_y = (float)(4 - cy);
+            hi_y = (float)(H - 4 - cy);
+            ref_base = (cy - half + ref_dy) * ref_pitch + (cx - half + ref_dx);
+            if (op == 1) {
+                tile_ok = req->tile_ok != 0;
+                tx0 = req->tx0;
+                ty0 = req->ty0;
+                float Wp[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) Wp[k] = req->Wp[k];
+                const int lo = warp * per, hi = min(K, lo + per);
+                gbits[warp * 32 + lane] = lo < hi ? sample_part(Wp, lo, hi) : Mask(0);
+            } else {
+                coarse_warp(warp * 32 + lane);
+            }
+            coop_bar();  // results in shared memory
+        }
+    }
+
+    // COOP, the driver: post a request; the caller's own share follows.
+    __device__ __forceinline__ void coop_post(int op, const float* Wp) {
+        if (lane == 0) {
+            req->op = op;
+            req->cx = cx;
+            req->cy = cy;
+            req->tile_ok = tile_ok ? 1 : 0;
+            req->tx0 = tx0;
+            req->ty0 = ty0;
+            if (Wp)
+                for (int k = 0; k < 6; ++k) req->Wp[k] = Wp[k];
+        }
+        __syncwarp();
+        coop_bar();
+    }
+
     // sample_warped_subset (optimization_engine.cpp:191-269): every pixel's
     // value into vals, the valid ones (inside the guard, outside the Ghost
-    // Wall) flagged in `valid` and summed; returns their count. Four pixels'
-    // loads are issued before their stores.
+    // Wall) flagged in `valid` and summed in pixel order; returns their count.
     __device__ __forceinline__ int sample(const float Wp[6], float& sum, Mask& valid) {
         ensure_tile(Wp);
+        if constexpr (COOP) {
+            const int per = (K + kCoopWarps - 1) / kCoopWarps;
+            coop_post(1, Wp);
+            Mask g = sample_part(Wp, 0, min(K, per));
+            coop_bar();
+#pragma unroll
+            for (int w = 1; w < kCoopWarps; ++w) g |= gbits[w * 32 + lane];
+            valid = g & refok;
+            float part = 0.0f;
+            int cnt = 0;
+            for (int k = 0; k < K; ++k)
+                if ((valid >> k) & 1u) {
+                    part = part + vals[lane + 32 * k];
+                    ++cnt;
+                }
+            sum = wsum(part);
+            return wsum(cnt);
+        }
+
         float part = 0.0f;
         int cnt = 0;
         valid = 0;
@@ -1380,63 +1518,57 @@ struct WarpSolver {
         return res;
     }
 
-    // estimate_initial_guess (optimization_engine.cpp:120-179): one offset
-    // per lane at a time (8 each), sequential sums as the reference, then the
-    // first minimum in the reference's v-major order. Returns (u, v); the
-    // guess when no offset qualifies.
-    __device__ __forceinline__ float2 coarse(float gu, float gv) const {
-        int sampled = 0;
-        for (int i = 0; i < n; i += 9) ++sampled;
-        float best = 1e20f;
-        int best_idx = 1 << 30;
-        for (int j = 0; j < 8; ++j) {
-            const int idx = lane * 8 + j;  // increasing per lane: first minimum kept
-            const int v = -15 + 2 * (idx / 16), u = -15 + 2 * (idx % 16);
-            auto sample_at = [&](int i, float& rr, float& dd) {
-                const int row = i / dim, col = i - (i / dim) * dim;
-                const float rv = __ldg(refI + ref_base + row * ref_pitch + col);
-                if (rv < kGhost) return false;
-                const int x = cx + (col - half) + u, y = cy + (row - half) + v;
-                if (x < 4 || x > W - 5 || y < 4 || y > H - 5) return false;
-                rr = rv;
-                dd = __ldg(defI + (size_t)y * pitch + x);
-                return true;
-            };
-            int m = 0;
-            float mr = 0.0f, md = 0.0f;
-            for (int i = 0; i < n; i += 9) {
-                float rr, dd;
-                if (!sample_at(i, rr, dd)) continue;
-                mr = mr + rr;
-                md = md + dd;
-                ++m;
-            }
-            if (m < 3 || 2 * m < sampled) continue;
-            const float fm = (float)m;
-            mr = mr / fm;
-            md = md / fm;
-            float vr = 0.0f, vd = 0.0f;
-            for (int i = 0; i < n; i += 9) {
-                float rr, dd;
-                if (!sample_at(i, rr, dd)) continue;
-                vr = vr + (rr - mr) * (rr - mr);
-                vd = vd + (dd - md) * (dd - md);
-            }
-            const float sr = sqrtf(vr / fm), sd = sqrtf(vd / fm);
-            if (!(sr > 1e-5f) || !(sd > 1e-5f)) continue;
-            float score = 0.0f;
-            for (int i = 0; i < n; i += 9) {
-                float rr, dd;
-                if (!sample_at(i, rr, dd)) continue;
-                const float e = (rr - mr) / sr - (dd - md) / sd;
-                score = score + e * e;
-            }
-            score = score / fm;
-            if (score < best) {
-                best = score;
-                best_idx = idx;
-            }
+    // estimate_initial_guess (optimization_engine.cpp:120-179) for one offset
+    // (idx: v-major over the 16 x 16 grid of +-15 px in steps of 2) with the
+    // reference's sequential sums over every 9th subset pixel; 1e20 when the
+    // offset does not qualify.
+    __device__ __forceinline__ float coarse_score(int idx, int sampled) const {
+        const int v = -15 + 2 * (idx / 16), u = -15 + 2 * (idx % 16);
+        auto sample_at = [&](int i, float& rr, float& dd) {
+            const int row = i / dim, col = i - (i / dim) * dim;
+            const float rv = __ldg(refI + ref_base + row * ref_pitch + col);
+            if (rv < kGhost) return false;
+            const int x = cx + (col - half) + u, y = cy + (row - half) + v;
+            if (x < 4 || x > W - 5 || y < 4 || y > H - 5) return false;
+            rr = rv;
+            dd = __ldg(defI + (size_t)y * pitch + x);
+            return true;
+        };
+        int m = 0;
+        float mr = 0.0f, md = 0.0f;
+        for (int i = 0; i < n; i += 9) {
+            float rr, dd;
+            if (!sample_at(i, rr, dd)) continue;
+            mr = mr + rr;
+            md = md + dd;
+            ++m;
         }
+        if (m < 3 || 2 * m < sampled) return 1e20f;
+        const float fm = (float)m;
+        mr = mr / fm;
+        md = md / fm;
+        float vr = 0.0f, vd = 0.0f;
+        for (int i = 0; i < n; i += 9) {
+            float rr, dd;
+            if (!sample_at(i, rr, dd)) continue;
+            vr = vr + (rr - mr) * (rr - mr);
+            vd = vd + (dd - md) * (dd - md);
+        }
+        const float sr = sqrtf(vr / fm), sd = sqrtf(vd / fm);
+        if (!(sr > 1e-5f) || !(sd > 1e-5f)) return 1e20f;
+        float score = 0.0f;
+        for (int i = 0; i < n; i += 9) {
+            float rr, dd;
+            if (!sample_at(i, rr, dd)) continue;
+            const float e = (rr - mr) / sr - (dd - md) / sd;
+            score = score + e * e;
+        }
+        return score / fm;
+    }
+
+    // The warp's minimum over (best, idx): the lowest score, ties to the lower
+    // offset index (the reference's first minimum).
+    __device__ __forceinline__ static void argmin_warp(float& best, int& best_idx) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             const float os = __shfl_xor_sync(kFull, best, o);
@@ -1446,6 +1578,49 @@ struct WarpSolver {
                 best_idx = oi;
             }
         }
+    }
+
+    // COOP: offset idx on this thread; the warp's minimum into its slot.
+    __device__ __forceinline__ void coarse_warp(int idx) {
+        int sampled = 0;
+        for (int i = 0; i < n; i += 9) ++sampled;
+        float best = coarse_score(idx, sampled);
+        int best_idx = best < 1e20f ? idx : (1 << 30);
+        argmin_warp(best, best_idx);
+        if (lane == 0) cslots[warp] = make_float2(best, __int_as_float(best_idx));
+    }
+
+    // estimate_initial_guess: the first minimum in the reference's v-major
+    // order. One offset per lane at a time (8 each); with COOP one per thread
+    // of the block. Returns (u, v); the guess when no offset qualifies.
+    __device__ __forceinline__ float2 coarse(float gu, float gv) {
+        float best = 1e20f;
+        int best_idx = 1 << 30;
+        if constexpr (COOP) {
+            coop_post(2, nullptr);
+            coarse_warp(lane);
+            coop_bar();
+            for (int w = 0; w < kCoopWarps; ++w) {
+                const float2 c = cslots[w];
+                const int ci = __float_as_int(c.y);
+                if (c.x < best || (c.x == best && ci < best_idx)) {
+                    best = c.x;
+                    best_idx = ci;
+                }
+            }
+        } else {
+            int sampled = 0;
+            for (int i = 0; i < n; i += 9) ++sampled;
+            for (int j = 0; j < 8; ++j) {
+                const int idx = lane * 8 + j;  // increasing per lane: first minimum kept
+                const float score = coarse_score(idx, sampled);
+                if (score < best) {
+                    best = score;
+                    best_idx = idx;
+                }
+            }
+            argmin_warp(best, best_idx);
+        }
         if (best_idx < 256 && best < 1e20f)
             return make_float2((float)(-15 + 2 * (best_idx % 16)), (float)(-15 + 2 * (best_idx / 16)));
         return make_float2(gu, gv);
@@ -1454,8 +1629,8 @@ struct WarpSolver {
 
 // Set a warp's solver up for a launch: shared-memory arrays, launch
 // constants (copied out of the by-value argument block), tile state, barrier.
-template <bool SIX, class Mask, bool STAGE>
-__device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE>& s, unsigned char* smem, const StagedLayout& L,
+template <bool SIX, class Mask, bool STAGE, bool COOP>
+__device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>& s, unsigned char* smem, const StagedLayout& L,
                                              const CUtensorMap* tmap, const float* refI, const float* refGx,
                                              const float* refGy, const float* defI, int* err, int n, int dim,
                                              int pitch, int tw, int th, int W, int H, int min_valid, int lm,
@@ -1498,7 +1673,12 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE>& s, un
     s.tile_ok = false;
     s.tile_on = tw > 0;
     s.phase = 0;
-    if (lane == 0) mbar_init(s.bar, 1);
+    s.warp = (int)(threadIdx.x >> 5);
+    s.req = reinterpret_cast<CoopReq*>(smem + L.off_coop);
+    s.gbits = reinterpret_cast<Mask*>(smem + L.off_coop + 64);
+    s.cslots = reinterpret_cast<float2*>(smem + L.off_coop + 64 + kCoopWarps * 32 * 8);
+    // one barrier per block, set up by its first warp (the driver, with COOP)
+    if (threadIdx.x == 0) mbar_init(s.bar, 1);
     fence_proxy_async_smem();
     __syncwarp();
 }
@@ -1581,14 +1761,23 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
 // The rescue pass over the tasks the fast pass handed on, with every path of
 // calculate_deformation (optimization_engine.cpp:55-118): the coarse search
 // and 2-DOF Simplex of AUTO_SEARCH, masked iterations, and the 6-DOF Simplex
-// rescue of NO_SEARCH, keeping the better run.
+// rescue of NO_SEARCH, keeping the better run. A block of kCoopWarps warps
+// per task: warp 0 runs the task, and every evaluation's sampling (and the
+// coarse search's 256 offsets) is shared by all warps of the block. The
+// ordered reductions stay on warp 0, so the results are those of a single
+// warp. Every exit of the driver's loop posts "done", which is what ends the
+// other warps' loop.
 template <bool SIX>
-__global__ void __launch_bounds__(32, 1) rescue_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
-                                                       const StagedLayout L) {
+__global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const __grid_constant__ CUtensorMap tmap,
+                                                                         const SolveArgs a, const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
-    WarpSolver<SIX, uint64_t> s;
+    WarpSolver<SIX, uint64_t, true, true> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
                  a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+    if (s.warp != 0) {
+        s.coop_serve();
+        return;
+    }
     const int lane = s.lane, dim = s.dim, half = s.half;
     const int ntasks = *(volatile const int*)(a.queue + 2);
     int* const queue = a.queue + 1;
@@ -1655,18 +1844,19 @@ __global__ void __launch_bounds__(32, 1) rescue_kernel(const __grid_constant__ C
         }
         __syncwarp();
     }
+    s.coop_post(0, nullptr);  // done: the other warps leave their loop
 }
 
-// Blocks of one warp: as many as fit on the device at once (persistent),
-// at most `cap` (when positive) and at most one per task.
+// Blocks of `threads` threads: as many as fit on the device at once
+// (persistent), at most `cap` (when positive) and at most one per task.
 template <class K>
-cudaError_t one_wave(K kernel, size_t smem, long cap, long tasks, long& blocks) {
+cudaError_t one_wave(K kernel, size_t smem, long cap, long tasks, long& blocks, int threads = 32) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (e != cudaSuccess) return e;
     blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
     if (cap > 0 && blocks > cap) blocks = cap;
@@ -1701,11 +1891,13 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
         e = one_wave(fast, FL.bytes, 0, a.n_tasks, blocks);
         if (e != cudaSuccess) return e;
         fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
-        e = cudaFuncSetAttribute(rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, SL.bytes);
+        // the rescue pass: a block of kCoopWarps warps per task
+        const StagedLayout RL = staged_layout(a.n, a.tile_w, a.tile_h, true, true);
+        e = cudaFuncSetAttribute(coop_rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, RL.bytes);
         if (e != cudaSuccess) return e;
-        e = one_wave(rescue_kernel<SIX>, SL.bytes, cap, a.n_tasks, blocks);
+        e = one_wave(coop_rescue_kernel<SIX>, RL.bytes, cap, a.n_tasks, blocks, kCoopWarps * 32);
         if (e != cudaSuccess) return e;
-        rescue_kernel<SIX><<<(unsigned)blocks, 32, SL.bytes, st>>>(tmap, a, SL);
+        coop_rescue_kernel<SIX><<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tmap, a, RL);
         return cudaGetLastError();
     }
     e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
