@@ -145,43 +145,66 @@ __device__ __forceinline__ float interp6s(const float* base, int pitch, int xi, 
 }
 
 // The 6x6 FP64 helpers of the Hessian: Cholesky, explicit inverse, and the
-// scaled 1-norm reciprocal condition (src/math/hessian.hpp:40-52).
-static __device__ __noinline__ bool cholesky6(const double A[6][6], double L[6][6]) {
+// scaled 1-norm reciprocal condition (src/math/hessian.hpp:40-52). The `_r`
+// forms are fully unrolled, so their matrices live in registers; the
+// out-of-line forms copy their arguments in and out around them, for callers
+// that are short of registers. Both perform the same operations in the same
+// order.
+__device__ __forceinline__ bool cholesky6_r(const double (&A)[6][6], double (&L)[6][6]) {
+#pragma unroll
     for (int i = 0; i < 6; ++i)
+#pragma unroll
         for (int j = 0; j < 6; ++j) L[i][j] = 0.0;
+    bool ok = true;
+#pragma unroll
     for (int j = 0; j < 6; ++j) {
         double s = A[j][j];
+#pragma unroll
         for (int k = 0; k < j; ++k) s = s - L[j][k] * L[j][k];
-        if (!(s > 0.0) || !finite_d(s)) return false;
+        ok = ok && (s > 0.0) && finite_d(s);
         const double d = sqrt(s);
         L[j][j] = d;
+#pragma unroll
         for (int i = j + 1; i < 6; ++i) {
             double t = A[i][j];
+#pragma unroll
             for (int k = 0; k < j; ++k) t = t - L[i][k] * L[j][k];
             L[i][j] = t / d;
         }
+        if (!ok) return false;
     }
     return true;
 }
 
-static __device__ __noinline__ bool inverse6(const double A[6][6], double Ai[6][6]) {
+// Ai is written whenever the factorisation succeeds (factored), even when a
+// non-finite entry makes the result false.
+__device__ __forceinline__ bool inverse6_r(const double (&A)[6][6], double (&Ai)[6][6], bool& factored) {
     double L[6][6];
-    if (!cholesky6(A, L)) return false;
+    factored = cholesky6_r(A, L);
+    if (!factored) return false;
     double Li[6][6];
+#pragma unroll
     for (int i = 0; i < 6; ++i)
+#pragma unroll
         for (int j = 0; j < 6; ++j) Li[i][j] = 0.0;
+#pragma unroll
     for (int c = 0; c < 6; ++c) {
         Li[c][c] = 1.0 / L[c][c];
+#pragma unroll
         for (int i = c + 1; i < 6; ++i) {
             double t = 0.0;
+#pragma unroll
             for (int k = c; k < i; ++k) t = t + L[i][k] * Li[k][c];
             Li[i][c] = -t / L[i][i];
         }
     }
     bool ok = true;
+#pragma unroll
     for (int r = 0; r < 6; ++r)
+#pragma unroll
         for (int c = r; c < 6; ++c) {
             double t = 0.0;
+#pragma unroll
             for (int k = c; k < 6; ++k) t = t + Li[k][r] * Li[k][c];
             Ai[r][c] = t;
             Ai[c][r] = t;
@@ -190,19 +213,26 @@ static __device__ __noinline__ bool inverse6(const double A[6][6], double Ai[6][
     return ok;
 }
 
-static __device__ __noinline__ bool well_conditioned(const double H[6][6], int half) {
+__device__ __forceinline__ bool well_conditioned_r(const double (&H)[6][6], int half) {
     const double s = half > 1 ? 1.0 / (double)half : 1.0;
     const double d[6] = {1.0, 1.0, s, s, s, s};
     double Hn[6][6], Hi[6][6];
+    bool fin = true;
+#pragma unroll
     for (int r = 0; r < 6; ++r)
+#pragma unroll
         for (int c = 0; c < 6; ++c) {
             Hn[r][c] = (d[r] * H[r][c]) * d[c];
-            if (!finite_d(Hn[r][c])) return false;
+            fin = fin && finite_d(Hn[r][c]);
         }
-    if (!inverse6(Hn, Hi)) return false;
+    if (!fin) return false;
+    bool factored;
+    if (!inverse6_r(Hn, Hi, factored)) return false;
     double na = 0.0, ni = 0.0;
+#pragma unroll
     for (int c = 0; c < 6; ++c) {
         double a = 0.0, b = 0.0;
+#pragma unroll
         for (int r = 0; r < 6; ++r) {
             a = a + fabs(Hn[r][c]);
             b = b + fabs(Hi[r][c]);
@@ -213,7 +243,33 @@ static __device__ __noinline__ bool well_conditioned(const double H[6][6], int h
     return 1.0 / (na * ni) > (double)1e-6f;
 }
 
-static __device__ __noinline__ bool cond2x2_ok(const double H[6][6]) {
+static __device__ __noinline__ bool inverse6(const double A[6][6], double Ai[6][6]) {
+    double a[6][6], ai[6][6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) a[r][c] = A[r][c];
+    bool factored;
+    const bool ok = inverse6_r(a, ai, factored);
+    if (factored) {
+#pragma unroll
+        for (int r = 0; r < 6; ++r)
+#pragma unroll
+            for (int c = 0; c < 6; ++c) Ai[r][c] = ai[r][c];
+    }
+    return ok;
+}
+
+static __device__ __noinline__ bool well_conditioned(const double H[6][6], int half) {
+    double h[6][6];
+#pragma unroll
+    for (int r = 0; r < 6; ++r)
+#pragma unroll
+        for (int c = 0; c < 6; ++c) h[r][c] = H[r][c];
+    return well_conditioned_r(h, half);
+}
+
+__device__ __forceinline__ bool cond2x2_ok(const double (&H)[6][6]) {
     const double det = H[0][0] * H[1][1] - H[1][0] * H[0][1];
     const double nrm = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[1][0] * H[1][0] + H[1][1] * H[1][1];
     const double cond = fabs(det) > 1e-12 ? nrm / fabs(det) : 1.0e13;

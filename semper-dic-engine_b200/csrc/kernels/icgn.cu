@@ -1847,6 +1847,25 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
     s.coop_post(0, nullptr);  // done: the other warps leave their loop
 }
 
+// The dynamic shared-memory limit of a kernel, always set to the device's
+// opt-in maximum. The attribute belongs to the function for the whole
+// process, so a per-launch value would race between engines solving on other
+// threads: one thread's smaller setting would make another thread's larger
+// launch invalid. The occupancy still follows each launch's own size.
+template <class K>
+cudaError_t allow_max_smem(K kernel) {
+    int dev = 0, optin = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (e != cudaSuccess) return e;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, kernel);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes);
+}
+
 // Blocks of `threads` threads: as many as fit on the device at once
 // (persistent), at most `cap` (when positive) and at most one per task.
 template <class K>
@@ -1886,21 +1905,21 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
         if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31, false>;
         if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41, false>;
         const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, false);
-        e = cudaFuncSetAttribute(fast, cudaFuncAttributeMaxDynamicSharedMemorySize, FL.bytes);
+        e = allow_max_smem(fast);
         if (e != cudaSuccess) return e;
         e = one_wave(fast, FL.bytes, 0, a.n_tasks, blocks);
         if (e != cudaSuccess) return e;
         fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
         // the rescue pass: a block of kCoopWarps warps per task
         const StagedLayout RL = staged_layout(a.n, a.tile_w, a.tile_h, true, true);
-        e = cudaFuncSetAttribute(coop_rescue_kernel<SIX>, cudaFuncAttributeMaxDynamicSharedMemorySize, RL.bytes);
+        e = allow_max_smem(coop_rescue_kernel<SIX>);
         if (e != cudaSuccess) return e;
         e = one_wave(coop_rescue_kernel<SIX>, RL.bytes, cap, a.n_tasks, blocks, kCoopWarps * 32);
         if (e != cudaSuccess) return e;
         coop_rescue_kernel<SIX><<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tmap, a, RL);
         return cudaGetLastError();
     }
-    e = cudaFuncSetAttribute(solve_kernel<SIX, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = allow_max_smem(solve_kernel<SIX, false>);
     if (e != cudaSuccess) return e;
     e = one_wave(solve_kernel<SIX, false>, smem, cap, a.n_tasks, blocks);
     if (e != cudaSuccess) return e;

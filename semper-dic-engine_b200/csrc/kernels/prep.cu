@@ -204,26 +204,33 @@ __global__ void pool_finish_kernel(int nodes, int half, int lm, uint8_t* __restr
     if (node >= nodes || valid[node] != 2) return;
     double* o = Hs21 + (size_t)node * 21;
     double Hm[6][6], Hs[6][6];
+#pragma unroll
     for (int a = 0; a < 6; ++a)
+#pragma unroll
         for (int b = a; b < 6; ++b) {
             Hm[a][b] = o[tri21(a, b)];
             Hm[b][a] = Hm[a][b];
         }
     if (H21)
+#pragma unroll
         for (int k = 0; k < 21; ++k) H21[(size_t)node * 21 + k] = o[k];
-    const bool good = cond2x2_ok(Hm) && well_conditioned(Hm, half);
+    const bool good = cond2x2_ok(Hm) && well_conditioned_r(Hm, half);
     uint8_t v = good ? 1 : 0;
-    bool done = false;
+    bool done = false, factored = false;
     if (good && lm) {
         double Hd[6][6];
+#pragma unroll
         for (int a = 0; a < 6; ++a)
+#pragma unroll
             for (int b = 0; b < 6; ++b) Hd[a][b] = Hm[a][b];
         Hd[0][0] += (double)0.05f;
         Hd[1][1] += (double)0.05f;
-        if (well_conditioned(Hd, half) && inverse6(Hd, Hs)) done = true;
+        if (well_conditioned_r(Hd, half) && inverse6_r(Hd, Hs, factored)) done = true;
     }
-    if (good && !done && !inverse6(Hm, Hs)) v = 0;
+    if (good && !done && !inverse6_r(Hm, Hs, factored)) v = 0;
+#pragma unroll
     for (int a = 0; a < 6; ++a)
+#pragma unroll
         for (int b = a; b < 6; ++b) o[tri21(a, b)] = good ? Hs[a][b] : 0.0;
     valid[node] = v;
 }

@@ -37,6 +37,7 @@ def jobs():
 def test_batch_equals_lone_runs(jobs):
     b = sb.Batch(workers=3)
     got = b.run(jobs)
+    assert b.last_error == ""
     for j, (rc, pts, met) in zip(jobs, got):
         lrc, lpts, lmet = _lone(j)
         assert rc == lrc
@@ -52,6 +53,19 @@ def test_batch_independent_of_workers_and_order(jobs):
     b = list(reversed(sb.Batch(workers=5).run(rev)))
     for (ra, pa, ma), (rb, pb, mb) in zip(a, b):
         assert ra == rb and np.array_equal(pa, pb) and np.array_equal(ma[COUNT_SLOTS], mb[COUNT_SLOTS])
+
+
+def test_many_workers_mixed_subsets():
+    """Engines on many threads launching the same kernels with different
+    shared-memory sizes (subsets 15 to 41) at once: every job as when run alone."""
+    js = sb.batch_jobs(24, seed=11, min_side=256, max_side=768)
+    one = sb.Batch(workers=1).run(js)
+    for _ in range(2):
+        b = sb.Batch(workers=12)
+        many = b.run(js)
+        assert b.last_error == ""
+        for (ra, pa, _), (rb, pb, _) in zip(one, many):
+            assert ra == rb and np.array_equal(pa, pb)
 
 
 def test_empty_batch():
