@@ -34,6 +34,14 @@ SEMPER_C_API void* semper_b200_stream(semper_engine* eng);
    launched]. Returns 0, or -3 for a NULL handle. */
 SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], long long counts[5]);
 
+/* Where the last semper_incremental_process call spent its time (host wall
+   clock, ms): out[0] the whole call, [1] its full-field solves, [2] its
+   anchor matches, [3] the material-mask warp, [4] the reference adoption,
+   [5] the packing of the carried field; [6] anchor matches made, [7] solves
+   run; then the device phases of its last solve as semper_b200_last_timings
+   gives them ([8..15]). For measurement. Returns 0, or -3 for a NULL handle. */
+SEMPER_C_API int semper_b200_incremental_profile(semper_incremental* inc, double out[16]);
+
 /* A global-motion model for the following runs on this handle: a 3x3
    homography, reference -> deformed, row-major (the role of the reference's
    AKAZE front end, src/pipeline/full_field_anchors.cpp:204-279). NULL clears

@@ -2,6 +2,7 @@
 // incremental_core.hpp, every solve, adoption and packing on the device.
 #include "incremental.hpp"
 
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
@@ -38,9 +39,14 @@ semper_inc::IncParams from_params(const Params& q) {
     return p;
 }
 
+double ms_since(std::chrono::steady_clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+}
+
 // The solver backend of the session: the device engine.
 struct DeviceBackend {
     Engine& e;
+    FrameProfile prof;
 
     int validate(semper_inc::IncParams& p, int W, int H) {
         Params q = to_params(p);
@@ -56,7 +62,10 @@ struct DeviceBackend {
             float* metrics, int metrics_len, const std::function<void(int)>& progress,
             semper_inc::SolveCapture* cap) {
         Capture c;
+        const auto t0 = std::chrono::steady_clock::now();
         const int rc = e.run(def, mask, to_params(p), out, capacity, metrics, metrics_len, nullptr, progress, &c);
+        prof.run += ms_since(t0);
+        prof.runs++;
         if (rc < 0) return rc;
         cap->gridW = c.gridW;
         cap->gridH = c.gridH;
@@ -76,24 +85,41 @@ struct DeviceBackend {
         cap->median_rejected = c.median_rejected;
         return rc;
     }
-    int adopt(const uint8_t* mask) { return e.adopt_last_deformed(mask); }
+    int adopt(const uint8_t* mask) {
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = e.adopt_last_deformed(mask);
+        prof.adopt += ms_since(t0);
+        return rc;
+    }
     int pack(const semper_inc::GridGeom& g, int window, const std::vector<float>& u, const std::vector<float>& v,
              const std::vector<float>& corr, const std::vector<unsigned char>& solved, float* out, int capacity) {
-        return e.pack_field(g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, window, u.data(), v.data(), corr.data(),
-                            solved.data(), out, capacity);
+        const auto t0 = std::chrono::steady_clock::now();
+        const int rc = e.pack_field(g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, window, u.data(), v.data(),
+                                    corr.data(), solved.data(), out, capacity);
+        prof.pack += ms_since(t0);
+        return rc;
     }
     semper_inc::Rect warp_mask(const std::vector<uint8_t>& mask0, int W, int H, const semper_inc::GridGeom& g,
                                const semper_inc::MaskWarpPlan& p, std::vector<uint8_t>& out) {
+        const auto t0 = std::chrono::steady_clock::now();
         out.resize((size_t)W * H);
         int box[4] = {0, 0, 0, 0};
         if (e.warp_mask(mask0.data(), W, H, g.gridW, g.gridH, g.rect_x, g.rect_y, g.step, p.U.data(), p.V.data(),
                         p.X0, p.X1, p.Y0, p.Y1, p.per_px, out.data(), box) != 0)
             throw std::runtime_error("mask warp");
+        prof.warp_mask += ms_since(t0);
         return semper_inc::Rect{box[0], box[1], box[2], box[3]};
     }
     bool match_anchor(const semper_inc::CoastAnchor& a, int subset, bool six, float gx, float gy, float max_shift,
                       float& x, float& y, float& corr) {
         // guess for the centre pixel: the node's guess less its offset from it
+        const auto t0 = std::chrono::steady_clock::now();
+        prof.matches++;
+        struct Add {
+            double& m;
+            std::chrono::steady_clock::time_point t;
+            ~Add() { m += ms_since(t); }
+        } add{prof.match, t0};
         const PatchSolve r = e.solve_patch(a.patch.data(), a.size, a.ax, a.ay, gx - a.dx - (float)a.ax,
                                            gy - a.dy - (float)a.ay, subset, six);
         if (!r.initialized) return false;
@@ -106,7 +132,7 @@ struct DeviceBackend {
 
 struct IncrementalSession::Impl {
     Engine engine;
-    DeviceBackend backend{engine};
+    DeviceBackend backend{engine, FrameProfile{}};
     semper_inc::IncrementalCore<DeviceBackend> core{backend};
 };
 
@@ -131,10 +157,15 @@ int IncrementalSession::init(const uint8_t* ref, int w, int h, const uint8_t* ma
     return impl_->core.init(ref, w, h, mask, from_params(p), update_interval);
 }
 
+const FrameProfile& IncrementalSession::last_profile() const { return impl_->backend.prof; }
+
 int IncrementalSession::process(const uint8_t* def, float* out, int capacity, float* metrics, int metrics_len,
                                 Progress progress, FrameInfo* info) {
     semper_inc::FrameInfo fi;
+    impl_->backend.prof = FrameProfile{};
+    const auto t0 = std::chrono::steady_clock::now();
     const int rc = impl_->core.process(def, out, capacity, metrics, metrics_len, progress, &fi);
+    impl_->backend.prof.total = ms_since(t0);
     if (info) {
         info->reference_frame = fi.reference_frame;
         info->reference_updated = fi.reference_updated;

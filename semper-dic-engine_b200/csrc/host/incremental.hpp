@@ -17,6 +17,13 @@ struct FrameInfo {
     int lost_this_frame = 0;
 };
 
+// Host wall time of the last process() call by step, ms, and the number of
+// anchor matches it made (measurement only).
+struct FrameProfile {
+    double total = 0, run = 0, match = 0, warp_mask = 0, adopt = 0, pack = 0;
+    int matches = 0, runs = 0;
+};
+
 class IncrementalSession {
 public:
     IncrementalSession();
@@ -30,6 +37,7 @@ public:
     bool initialized() const;
     int frames_processed() const;
     Engine& engine();
+    const FrameProfile& last_profile() const;
 
     struct Impl;
 

@@ -228,6 +228,16 @@ SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], lo
     return 0;
 }
 
+SEMPER_C_API int semper_b200_incremental_profile(semper_incremental* inc, double out[16]) {
+    if (inc == nullptr || out == nullptr) return SEMPER_ERR_INIT;
+    const semper_b200::FrameProfile& f = inc->session->last_profile();
+    const semper_b200::PhaseTimes& t = inc->session->engine().last_times();
+    const double v[16] = {f.total, f.run, f.match, f.warp_mask, f.adopt, f.pack, (double)f.matches, (double)f.runs,
+                          t.prep, t.pool, t.seed, t.mesh, t.path_a, t.path_b, t.strain, t.total};
+    for (int i = 0; i < 16; ++i) out[i] = v[i];
+    return 0;
+}
+
 SEMPER_C_API int semper_b200_set_global_model(semper_engine* eng, const double* h9) {
     if (eng == nullptr) return SEMPER_ERR_INIT;
     HandleCall call(eng->busy);

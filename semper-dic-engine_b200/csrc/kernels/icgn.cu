@@ -858,6 +858,11 @@ struct WarpSolver {
     // the TMA tile (warp-uniform)
     int tx0, ty0;
     bool tile_ok, tile_on;
+    // every corner of the warped subset inside the 4 px guard with 0.01 px to
+    // spare (so every sample is inside it too, rounding included); set by
+    // ensure_tile
+    bool all_in;
+    Mask fullmask;  // bit k set when pixel lane + 32 k exists
     unsigned phase;
     // the task
     int cx, cy, ref_base, ghost;
@@ -945,6 +950,7 @@ struct WarpSolver {
     // The tile must cover every sample support of the warped subset: stage a
     // new box with TMA when the warp has left the current one.
     __device__ __forceinline__ void ensure_tile(const float Wp[6]) {
+        all_in = false;
         if (!tile_on) return;
         const float h = (float)half;
         float mnx = 0.0f, mxx = 0.0f, mny = 0.0f, mxy = 0.0f;
@@ -964,6 +970,8 @@ struct WarpSolver {
             tile_ok = false;
             return;
         }
+        all_in = mnx + 0.5f >= lo_x + 0.01f && mxx + 0.5f < hi_x - 0.01f && mny + 0.5f >= lo_y + 0.01f &&
+                 mxy + 0.5f < hi_y - 0.01f;
         const int lo_tap = SIX ? 3 : 2, hi_tap = SIX ? 4 : 3;
         const int x_lo = cx + (int)floorf(mnx) - lo_tap, x_hi = cx + (int)floorf(mxx) + hi_tap;
         const int y_lo = cy + (int)floorf(mny) - lo_tap, y_hi = cy + (int)floorf(mxy) + hi_tap;
@@ -1107,6 +1115,43 @@ struct WarpSolver {
                 }
             sum = wsum(part);
             return wsum(cnt);
+        }
+        if constexpr (!STAGE && !COOP) {
+            // the fast pass's common case: every sample inside the guard and
+            // the tile, no Ghost Wall pixel, so every pixel is valid and the
+            // per-pixel tests are skipped (same values, same order of sums)
+            if (all_in && tile_ok && ghost == 0) {
+                float part = 0.0f;
+                int row = row0, col = col0;
+                for (int k0 = 0; k0 < K; k0 += 4) {
+                    float v[4];
+                    int ii[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int k = k0 + u;
+                        ii[u] = lane + 32 * k;
+                        v[u] = 0.0f;
+                        if (k < K && ii[u] < n) {
+                            const float ox = (float)(col - half), oy = (float)(row - half);
+                            const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
+                            const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
+                            const float flx = floorf(fx), fly = floorf(fy);
+                            const int lx = cx + (int)flx - tx0, ly = cy + (int)fly - ty0;
+                            v[u] = SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly)
+                                       : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
+                            part = part + v[u];
+                        }
+                        advance(row, col);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+                        if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
+                }
+                __syncwarp();
+                valid = fullmask;
+                sum = wsum(part);
+                return n;
+            }
         }
 
         float part = 0.0f;
@@ -1672,6 +1717,10 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
     s.tx0 = s.ty0 = 0;
     s.tile_ok = false;
     s.tile_on = tw > 0;
+    s.all_in = false;
+    s.fullmask = 0;
+    for (int k = 0; k < s.K; ++k)
+        if (lane + 32 * k < n) s.fullmask |= Mask(1) << k;
     s.phase = 0;
     s.warp = (int)(threadIdx.x >> 5);
     s.req = reinterpret_cast<CoopReq*>(smem + L.off_coop);

@@ -38,7 +38,7 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
                "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion",
                "semper_b200_batch_create", "semper_b200_batch_destroy", "semper_b200_batch_run",
-               "semper_b200_batch_last_error"]
+               "semper_b200_batch_last_error", "semper_b200_incremental_profile"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -109,6 +109,7 @@ def lib():
         L.semper_b200_batch_create.restype = _vp
         L.semper_b200_batch_destroy.argtypes = [_vp]
         L.semper_b200_batch_run.argtypes = [_vp, ctypes.POINTER(BatchJob), ctypes.c_int32]
+        L.semper_b200_incremental_profile.argtypes = [_vp, _f64p]
         L.semper_b200_batch_last_error.argtypes = [_vp]
         L.semper_b200_batch_last_error.restype = ctypes.c_char_p
         L.semper_b200_last_global_motion.argtypes = [_vp, _f64p]
@@ -348,6 +349,14 @@ class Incremental:
         rc = lib().semper_incremental_process(self._h, _p(d, _u8p), d.size, _p(out, _f32p), capacity,
                                               _p(met, _f32p), metrics_len, ctypes.byref(info), PROGRESS_CB(), None)
         return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info
+
+    def profile(self) -> dict:
+        """Where the last process() call spent its time (semper_b200_incremental_profile)."""
+        o = np.zeros(16, np.float64)
+        lib().semper_b200_incremental_profile(self._h, _p(o, _f64p))
+        keys = ["total", "run", "match", "warp_mask", "adopt", "pack", "matches", "runs",
+                "prep", "pool", "seed", "mesh", "path_a", "path_b", "strain", "solve_total"]
+        return dict(zip(keys, map(float, o)))
 
 
 def version() -> str:
