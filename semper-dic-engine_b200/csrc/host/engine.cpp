@@ -726,10 +726,12 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
 
         // ---------------------------------------------------------------- grid + pool
         const auto t_prepass = clk::now();
-        const std::vector<uint8_t> mk = mask ? std::vector<uint8_t>(mask, mask + (size_t)W * H) : std::vector<uint8_t>();
+        // the cached grid and pool hold for this mask (compared in place: no copy on a hit)
+        const size_t mask_n = mask ? (size_t)W * H : 0;
+        const bool same_mask = mask_key.size() == mask_n && (mask_n == 0 || std::memcmp(mask_key.data(), mask, mask_n) == 0);
         const bool cached = grid_valid && key.rect_x == params.rect_x && key.rect_y == params.rect_y &&
                             key.rect_w == params.rect_w && key.rect_h == params.rect_h && key.step == params.step &&
-                            key.subset_size == params.subset_size && mask_key == mk && gridW == gW && gridH == gH;
+                            key.subset_size == params.subset_size && same_mask && gridW == gW && gridH == gH;
         if (!cached) {
             grid_valid = false;
             skip.ensure(NG);
@@ -758,7 +760,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             sync();
             poll_cancel();
             key = params;
-            mask_key = mk;
+            mask_key.assign(mask, mask + mask_n);
             gridW = gW;
             gridH = gH;
             total_valid = nv;

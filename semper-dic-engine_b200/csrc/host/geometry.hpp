@@ -71,25 +71,59 @@ inline std::vector<Tri> delaunay(const std::vector<Pt>& pts) {
     X[n + 1] = mid + 20 * span; Y[n + 1] = mid - 20 * span;
     X[n + 2] = mid; Y[n + 2] = mid + 20 * span;
 
+    // Each triangle carries its circumcircle in double precision, a filter
+    // only: a point farther than the radius (with a wide margin) cannot be
+    // inside, and every other candidate gets the exact integer test. The
+    // triangles found are those of the exact test alone.
+    struct Circ {
+        double x, y, r2;  // r2 < 0: degenerate, always tested
+    };
+    auto circ_of = [&](const Tri& T) {
+        const double ax = (double)X[T.a], ay = (double)Y[T.a], bx = (double)X[T.b], by = (double)Y[T.b];
+        const double cx = (double)X[T.c], cy = (double)Y[T.c];
+        const double d = 2.0 * (ax * (by - cy) + bx * (cy - ay) + cx * (ay - by));
+        if (!(std::fabs(d) > 0.0)) return Circ{0.0, 0.0, -1.0};
+        const double a2 = ax * ax + ay * ay, b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
+        const double ux = (a2 * (by - cy) + b2 * (cy - ay) + c2 * (ay - by)) / d;
+        const double uy = (a2 * (cx - bx) + b2 * (ax - cx) + c2 * (bx - ax)) / d;
+        return Circ{ux, uy, (ax - ux) * (ax - ux) + (ay - uy) * (ay - uy)};
+    };
     std::vector<Tri> tris;
+    std::vector<Circ> circs;
     tris.push_back({n, n + 1, n + 2});
+    circs.push_back(circ_of(tris.back()));
     std::vector<char> bad;
+    std::vector<int> bads;
     struct Edge { int a, b; };
     std::vector<Edge> poly;
+    std::vector<Tri> keep;
+    std::vector<Circ> keepc;
     for (int p = 0; p < n; ++p) {
         bad.assign(tris.size(), 0);
+        bads.clear();
+        const double px = (double)X[p], py = (double)Y[p];
         for (size_t t = 0; t < tris.size(); ++t) {
+            const Circ& C = circs[t];
+            if (C.r2 >= 0.0) {
+                const double dx = px - C.x, dy = py - C.y;
+                if (dx * dx + dy * dy > C.r2 * (1.0 + 1e-7) + 1.0) continue;
+            }
             const Tri& T = tris[t];
-            if (incircle_i(X[T.a], Y[T.a], X[T.b], Y[T.b], X[T.c], Y[T.c], X[p], Y[p]) > 0) bad[t] = 1;
+            if (incircle_i(X[T.a], Y[T.a], X[T.b], Y[T.b], X[T.c], Y[T.c], X[p], Y[p]) > 0) {
+                bad[t] = 1;
+                bads.push_back((int)t);
+            }
         }
+        // the cavity's boundary: the bad triangles' edges that no other bad
+        // triangle shares
         poly.clear();
-        for (size_t t = 0; t < tris.size(); ++t) {
-            if (!bad[t]) continue;
+        for (const int t : bads) {
             const int e[3][2] = {{tris[t].a, tris[t].b}, {tris[t].b, tris[t].c}, {tris[t].c, tris[t].a}};
             for (auto& ed : e) {
                 bool shared = false;
-                for (size_t u = 0; u < tris.size() && !shared; ++u) {
-                    if (u == t || !bad[u]) continue;
+                for (size_t k = 0; k < bads.size() && !shared; ++k) {
+                    const int u = bads[k];
+                    if (u == t) continue;
                     const int f[3][2] = {{tris[u].a, tris[u].b}, {tris[u].b, tris[u].c}, {tris[u].c, tris[u].a}};
                     for (auto& fd : f)
                         if ((fd[0] == ed[1] && fd[1] == ed[0]) || (fd[0] == ed[0] && fd[1] == ed[1])) shared = true;
@@ -97,16 +131,23 @@ inline std::vector<Tri> delaunay(const std::vector<Pt>& pts) {
                 if (!shared) poly.push_back({ed[0], ed[1]});
             }
         }
-        std::vector<Tri> keep;
-        keep.reserve(tris.size() + poly.size());
+        keep.clear();
+        keepc.clear();
         for (size_t t = 0; t < tris.size(); ++t)
-            if (!bad[t]) keep.push_back(tris[t]);
+            if (!bad[t]) {
+                keep.push_back(tris[t]);
+                keepc.push_back(circs[t]);
+            }
         for (const Edge& e : poly) {
             // A point on an existing edge of a bad triangle forms a flat
             // triangle with it; leave that one out.
-            if (orient_i(X[e.a], Y[e.a], X[e.b], Y[e.b], X[p], Y[p]) > 0) keep.push_back({e.a, e.b, p});
+            if (orient_i(X[e.a], Y[e.a], X[e.b], Y[e.b], X[p], Y[p]) > 0) {
+                keep.push_back({e.a, e.b, p});
+                keepc.push_back(circ_of(keep.back()));
+            }
         }
         tris.swap(keep);
+        circs.swap(keepc);
     }
     for (const Tri& t : tris) {
         if (t.a >= n || t.b >= n || t.c >= n) continue;

@@ -916,22 +916,33 @@ public:
         if (will_update) {
             const int before = (ref_index_ == 0) ? fi.frame0_points : alive_count();
             std::vector<float> coast_travel = coast_travel_;
-            std::map<size_t, CoastAnchor> anchors = anchors_;
+            // the anchors this update drops and refreshes, applied in place once
+            // the new reference is adopted (a failed adoption leaves them as
+            // they were)
+            std::vector<size_t> drop, refresh;
             for (size_t i = 0; i < n0; ++i) {
                 coast_travel[i] = (carried[i] && !valid[i]) ? coast_travel[i] + coast_step[i] : 0.0f;
                 if (!carried[i] || (valid[i] && need[i] == AnchorNeed::kDrop)) {
-                    anchors.erase(i);
+                    if (anchors_.count(i)) drop.push_back(i);
                 } else if (valid[i] && need[i] == AnchorNeed::kRefresh) {
-                    CoastAnchor a;
-                    if (make_anchor(def, width_, height_, (float)(g0.rect_x + (int)(i % g0.gridW) * g0.step) + U[i],
-                                    (float)(g0.rect_y + (int)(i / g0.gridW) * g0.step) + V[i], subset_size, a))
-                        anchors[i] = std::move(a);
+                    refresh.push_back(i);
                 }
             }
             NextReference next = prepare_reference(U, V, carried);
             if (b_.adopt(next.mask_k.data()) != 0) return -3;
+            for (const size_t i : drop) anchors_.erase(i);
+            for (const size_t i : refresh) {
+                const float ax = (float)(g0.rect_x + (int)(i % g0.gridW) * g0.step) + U[i];
+                const float ay = (float)(g0.rect_y + (int)(i / g0.gridW) * g0.step) + V[i];
+                const auto it = anchors_.find(i);
+                if (it != anchors_.end()) {
+                    make_anchor(def, width_, height_, ax, ay, subset_size, it->second);  // unchanged on failure
+                } else {
+                    CoastAnchor a;
+                    if (make_anchor(def, width_, height_, ax, ay, subset_size, a)) anchors_.emplace(i, std::move(a));
+                }
+            }
             coast_travel_.swap(coast_travel);
-            anchors_.swap(anchors);
             Ubase_.swap(next.Ubase);
             Vbase_.swap(next.Vbase);
             alive_.swap(next.alive);
