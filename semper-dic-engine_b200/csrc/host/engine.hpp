@@ -38,12 +38,17 @@ struct DevBuf {
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
+    // Room for count elements. A buffer that must grow gets half as much again
+    // as it had (or count, when more): sizes that creep up frame by frame
+    // (an incremental session's grid follows the material) then reallocate a
+    // few times, not every frame; cudaFree waits for the whole device.
     void ensure(size_t count) {
         if (count <= n && p) return;
+        size_t want = count == 0 ? 1 : count;
+        if (p && n + n / 2 > want) want = n + n / 2;
         release();
-        if (count == 0) count = 1;
-        check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
-        n = count;
+        check(cudaMalloc(&p, want * sizeof(T)), "cudaMalloc");
+        n = want;
     }
     void release() {
         if (p) cudaFree(p);
