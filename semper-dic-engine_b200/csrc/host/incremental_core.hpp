@@ -796,7 +796,7 @@ public:
         std::vector<unsigned char> valid(n0, 0), carried(n0, 0);
         std::vector<float> coast_step(n0, 0.0f);
         std::vector<AnchorNeed> need(n0, AnchorNeed::kKeep);
-        int coasting = 0, written = 0, frame0_points = frame0_points_;
+        int written = 0, frame0_points = frame0_points_;
         const int subset_size = params_.subset_size;
         const float max_travel = kIncCoastMaxTravelSubsets * (float)subset_size;
         auto carry = [&](size_t i, float du, float dv) {
@@ -806,7 +806,6 @@ public:
             V[i] = Vbase_[i] + dv;
             carried[i] = 1;
             coast_step[i] = travel;
-            coasting++;
         };
         auto coast = [&](size_t i, const NodeField& inc, float px, float py) {
             if (px < 0.0f || py < 0.0f || px > (float)(width_ - 1) || py > (float)(height_ - 1)) return;
@@ -845,7 +844,7 @@ public:
                 // nothing of this reference's grid can be solved: the nodes are dropped
                 fi.lost_this_frame = alive_count();
                 std::fill(alive_.begin(), alive_.end(), 0);
-                anchors_.clear();
+                for (CoastAnchor& a : anchors_) a.size = 0;
                 return nothing_to_follow(fi, metrics, metrics_len, progress, info);
             }
             if (rc < 0) return rc;
@@ -853,46 +852,66 @@ public:
             const GapDistance gd = gap_distance(inc);
             std::vector<float> gu(n0, 0.0f), gv(n0, 0.0f), gcorr(n0, kCorrInvalid);
             std::vector<unsigned char> gsolved(n0, 0);
-            for (int gy = 0; gy < g0.gridH; ++gy)
-                for (int gx = 0; gx < g0.gridW; ++gx) {
-                    const size_t i = (size_t)gy * g0.gridW + gx;
-                    const float x = (float)(g0.rect_x + gx * g0.step), y = (float)(g0.rect_y + gy * g0.step);
-                    if (!alive_[i]) continue;
-                    const float px = x + Ubase_[i], py = y + Vbase_[i];
-                    const IncrementSample smp = sample_increment(inc, px, py);
-                    if (!smp.ok) {
-                        coast(i, inc, px, py);
+            // Every node's own step depends on that node alone, so the nodes run
+            // in parallel; the anchor matches (device solves) then run one by
+            // one in node order.
+            enum : unsigned char { kNone, kValid, kMatch };
+            std::vector<unsigned char> state(n0, kNone), taylor(n0, 0);
+            std::vector<float> ncorr(n0, 0.0f);
+#pragma omp parallel for schedule(static)
+            for (long li = 0; li < (long)n0; ++li) {
+                const size_t i = (size_t)li;
+                if (!alive_[i]) continue;
+                const int gx = (int)(i % g0.gridW), gy = (int)(i / g0.gridW);
+                const float x = (float)(g0.rect_x + gx * g0.step), y = (float)(g0.rect_y + gy * g0.step);
+                const float px = x + Ubase_[i], py = y + Vbase_[i];
+                const IncrementSample smp = sample_increment(inc, px, py);
+                if (!smp.ok) {
+                    coast(i, inc, px, py);
+                    continue;
+                }
+                U[i] = Ubase_[i] + smp.u;
+                V[i] = Vbase_[i] + smp.v;
+                ncorr[i] = smp.corr;
+                taylor[i] = smp.taylor ? 1 : 0;
+                need[i] = anchor_need(inc, gd, px, py, subset_size);
+                if (coast_travel_[i] > trusted_travel) {
+                    // confirmed only by a direct match of its subset from where it was last clean
+                    if (need[i] == AnchorNeed::kKeep || anchor_of(i) == nullptr) {
+                        carried[i] = 1;
                         continue;
                     }
-                    U[i] = Ubase_[i] + smp.u;
-                    V[i] = Vbase_[i] + smp.v;
-                    float corr = smp.corr;
-                    need[i] = anchor_need(inc, gd, px, py, subset_size);
-                    if (coast_travel_[i] > trusted_travel) {
-                        // confirmed only by a direct match of its subset from where it was last clean
-                        const auto a = anchors_.find(i);
-                        const float max_shift =
-                            std::max(kIncReanchorMinShiftPx, kIncReanchorMaxShiftFraction * coast_travel_[i]);
-                        float mx = 0.0f, my = 0.0f;
-                        if (need[i] == AnchorNeed::kKeep || a == anchors_.end() ||
-                            !b_.match_anchor(a->second, subset_size, params_.six, x + U[i], y + V[i], max_shift, mx,
-                                             my, corr)) {
-                            carried[i] = 1;
-                            coasting++;
-                            continue;
-                        }
-                        U[i] = mx - x;
-                        V[i] = my - y;
-                        reanchored++;
-                    }
-                    valid[i] = 1;
-                    carried[i] = 1;
-                    if (smp.taylor) fi.taylor_fallbacks++;
-                    gu[i] = U[i];
-                    gv[i] = V[i];
-                    gcorr[i] = corr;
-                    gsolved[i] = 1;
+                    state[i] = kMatch;
+                    continue;
                 }
+                state[i] = kValid;
+            }
+            for (size_t i = 0; i < n0; ++i) {
+                if (state[i] == kMatch) {
+                    const float x = (float)(g0.rect_x + (int)(i % g0.gridW) * g0.step);
+                    const float y = (float)(g0.rect_y + (int)(i / g0.gridW) * g0.step);
+                    const float max_shift =
+                        std::max(kIncReanchorMinShiftPx, kIncReanchorMaxShiftFraction * coast_travel_[i]);
+                    float mx = 0.0f, my = 0.0f;
+                    if (!b_.match_anchor(*anchor_of(i), subset_size, params_.six, x + U[i], y + V[i], max_shift, mx,
+                                         my, ncorr[i])) {
+                        carried[i] = 1;
+                        continue;
+                    }
+                    U[i] = mx - x;
+                    V[i] = my - y;
+                    reanchored++;
+                } else if (state[i] != kValid) {
+                    continue;
+                }
+                valid[i] = 1;
+                carried[i] = 1;
+                if (taylor[i]) fi.taylor_fallbacks++;
+                gu[i] = U[i];
+                gv[i] = V[i];
+                gcorr[i] = ncorr[i];
+                gsolved[i] = 1;
+            }
             written = b_.pack(g0, params_.strain_window, gu, gv, gcorr, gsolved, output, output_capacity);
             if (written < 0) return written;
         }
@@ -923,24 +942,23 @@ public:
             for (size_t i = 0; i < n0; ++i) {
                 coast_travel[i] = (carried[i] && !valid[i]) ? coast_travel[i] + coast_step[i] : 0.0f;
                 if (!carried[i] || (valid[i] && need[i] == AnchorNeed::kDrop)) {
-                    if (anchors_.count(i)) drop.push_back(i);
+                    if (anchor_of(i)) drop.push_back(i);
                 } else if (valid[i] && need[i] == AnchorNeed::kRefresh) {
                     refresh.push_back(i);
                 }
             }
             NextReference next = prepare_reference(U, V, carried);
             if (b_.adopt(next.mask_k.data()) != 0) return -3;
-            for (const size_t i : drop) anchors_.erase(i);
-            for (const size_t i : refresh) {
+            if (anchors_.size() < n0) anchors_.resize(n0);
+            for (const size_t i : drop) anchors_[i].size = 0;
+            // each node's anchor is its own slot: the copies run in parallel; a
+            // patch that does not fit leaves the slot as it was
+#pragma omp parallel for schedule(static)
+            for (long k = 0; k < (long)refresh.size(); ++k) {
+                const size_t i = refresh[(size_t)k];
                 const float ax = (float)(g0.rect_x + (int)(i % g0.gridW) * g0.step) + U[i];
                 const float ay = (float)(g0.rect_y + (int)(i / g0.gridW) * g0.step) + V[i];
-                const auto it = anchors_.find(i);
-                if (it != anchors_.end()) {
-                    make_anchor(def, width_, height_, ax, ay, subset_size, it->second);  // unchanged on failure
-                } else {
-                    CoastAnchor a;
-                    if (make_anchor(def, width_, height_, ax, ay, subset_size, a)) anchors_.emplace(i, std::move(a));
-                }
+                make_anchor(def, width_, height_, ax, ay, subset_size, anchors_[i]);
             }
             coast_travel_.swap(coast_travel);
             Ubase_.swap(next.Ubase);
@@ -962,7 +980,6 @@ public:
             ref_reported_ = ref_reported;
             frame0_points_ = frame0_points;
         }
-        (void)coasting;
         (void)reanchored;
         if (info) *info = fi;
         return written;
@@ -1051,7 +1068,12 @@ private:
     std::vector<float> Ubase_, Vbase_;
     std::vector<unsigned char> alive_;
     std::vector<float> coast_travel_;
-    std::map<size_t, CoastAnchor> anchors_;
+    // the coasting anchor of each frame-0 node (size 0: none)
+    std::vector<CoastAnchor> anchors_;
+
+    const CoastAnchor* anchor_of(size_t i) const {
+        return i < anchors_.size() && anchors_[i].size > 0 ? &anchors_[i] : nullptr;
+    }
     int ref_index_ = 0, frames_since_update_ = 0, ref_reported_ = -1, adopted_reported_ = -1, frame_count_ = 0;
     IncParams params_k_;
     std::vector<uint8_t> mask_k_;
