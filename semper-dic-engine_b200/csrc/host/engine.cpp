@@ -250,15 +250,17 @@ struct Engine::Impl {
     cudaEvent_t ev[10];
 
     // Path B keeps two rounds in flight (full_field_path_b.cpp:148-412). Each
-    // in-flight round has its own slot: device buffers, scratch, a stream and
-    // pinned host staging, so the second round's solves run on the device
-    // while the first round is committed on the host.
+    // in-flight round has its own slot: a stream, scratch and host staging, so
+    // the second round's solves run on the device while the first round is
+    // committed on the host. A round's tasks and results stay in mapped pinned
+    // host memory that the kernels read and write directly (a round is at most
+    // a few hundred tasks): no copies to wait for between the rounds' kernels.
     struct Slot {
-        DevBuf<dic_task> tasks;
-        DevBuf<dic_result> results;
         DevBuf<int> q, deferred;
-        dic_task* h_tasks = nullptr;  // pinned
+        dic_task* h_tasks = nullptr;  // mapped pinned
         dic_result* h_results = nullptr;
+        dic_task* d_tasks = nullptr;  // their device addresses
+        dic_result* d_results = nullptr;
         size_t h_n = 0, n = 0;
         cudaStream_t s = nullptr;
         cudaEvent_t done = nullptr;
@@ -275,7 +277,7 @@ struct Engine::Impl {
     }
 
     // Enqueue one round's solves on slot k, after the work already on the
-    // engine stream (event `after`); results land in the slot's pinned buffer.
+    // engine stream (event `after`); results land in the slot's mapped buffer.
     void launch_round(int k, const std::vector<dic_task>& tk, const Params& p, cudaEvent_t after) {
         Slot& S = slots[k];
         if (!S.s) {
@@ -292,26 +294,23 @@ struct Engine::Impl {
                 S.h_tasks = nullptr;
                 S.h_results = nullptr;
                 S.h_n = 0;
-                check(cudaMallocHost(&S.h_tasks, S.n * sizeof(dic_task)), "pinned tasks");
-                check(cudaMallocHost(&S.h_results, S.n * sizeof(dic_result)), "pinned results");
-                S.h_n = S.n;
+                const size_t want = std::max<size_t>(S.n, 256);
+                check(cudaHostAlloc(&S.h_tasks, want * sizeof(dic_task), cudaHostAllocMapped), "mapped tasks");
+                check(cudaHostAlloc(&S.h_results, want * sizeof(dic_result), cudaHostAllocMapped), "mapped results");
+                check(cudaHostGetDevicePointer(&S.d_tasks, S.h_tasks, 0), "mapped tasks address");
+                check(cudaHostGetDevicePointer(&S.d_results, S.h_results, 0), "mapped results address");
+                S.h_n = want;
             }
-            S.tasks.ensure(std::max(S.tasks.n, S.n));
-            S.results.ensure(std::max(S.results.n, S.n));
             S.deferred.ensure(std::max(S.deferred.n, S.n));
             std::memcpy(S.h_tasks, tk.data(), S.n * sizeof(dic_task));
-            check(cudaMemcpyAsync(S.tasks.p, S.h_tasks, S.n * sizeof(dic_task), cudaMemcpyHostToDevice, S.s),
-                  "H2D round");
             dic::SolveArgs a = solve_args(p.subset_size, p.six);
-            a.tasks = S.tasks.p;
+            a.tasks = S.d_tasks;
             a.n_tasks = (int)S.n;
             a.n_tasks_dev = nullptr;
-            a.results = S.results.p;
+            a.results = S.d_results;
             a.queue = S.q.p;
             a.deferred = S.deferred.p;
             launched(2, dic::launch_solve(a, p.six ? 1 : 0, solve_grid((int)S.n), S.s), "round solve");
-            check(cudaMemcpyAsync(S.h_results, S.results.p, S.n * sizeof(dic_result), cudaMemcpyDeviceToHost, S.s),
-                  "D2H round");
         }
         check(cudaEventRecord(S.done, S.s), "slot record");
     }

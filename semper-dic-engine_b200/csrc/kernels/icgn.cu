@@ -29,7 +29,11 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
+#include <utility>
 
 #include "common.cuh"
 #include "dic_types.h"
@@ -1828,7 +1832,8 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
         return;
     }
     const int lane = s.lane, dim = s.dim, half = s.half;
-    const int ntasks = *(volatile const int*)(a.queue + 2);
+    // the tasks the fast pass handed on, or (rescue_all) every task
+    const int ntasks = a.rescue_all ? a.n_tasks : *(volatile const int*)(a.queue + 2);
     int* const queue = a.queue + 1;
     int polled = 0;
     for (;;) {
@@ -1837,7 +1842,7 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
         q = __shfl_sync(kFull, q, 0);
         if (q >= ntasks) break;
         if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
-        const int t = a.deferred[q];
+        const int t = a.rescue_all ? q : a.deferred[q];
         const dic_task T = a.tasks[t];
         dic_result out;
         out.u = out.v = out.ux = out.uy = out.vx = out.vy = 0.0f;
@@ -1901,31 +1906,69 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
 // process, so a per-launch value would race between engines solving on other
 // threads: one thread's smaller setting would make another thread's larger
 // launch invalid. The occupancy still follows each launch's own size.
+// Launch facts that do not change during the process (per device and
+// kernel): the opt-in attribute set, and each (kernel, threads, bytes)
+// occupancy. Looked up once, so that the many small solves of Path B rounds
+// pay no runtime queries.
+struct LaunchCache {
+    std::mutex m;
+    std::map<std::pair<int, const void*>, bool> smem_set;
+    std::map<std::tuple<int, const void*, int, size_t>, int> occupancy;
+    std::map<int, int> sms;
+};
+LaunchCache& launch_cache() {
+    static LaunchCache c;
+    return c;
+}
+
 template <class K>
 cudaError_t allow_max_smem(K kernel) {
     int dev = 0, optin = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    LaunchCache& c = launch_cache();
+    {
+        std::lock_guard<std::mutex> g(c.m);
+        if (c.smem_set.count({dev, (const void*)kernel})) return cudaSuccess;
+    }
     e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     if (e != cudaSuccess) return e;
     cudaFuncAttributes fa;
     e = cudaFuncGetAttributes(&fa, kernel);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                optin - (int)fa.sharedSizeBytes);
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> g(c.m);
+    c.smem_set[{dev, (const void*)kernel}] = true;
+    return cudaSuccess;
 }
-
-// Blocks of `threads` threads: as many as fit on the device at once
-// (persistent), at most `cap` (when positive) and at most one per task.
 template <class K>
 cudaError_t one_wave(K kernel, size_t smem, long cap, long tasks, long& blocks, int threads = 32) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
-    if (e != cudaSuccess) return e;
+    LaunchCache& c = launch_cache();
+    const auto key = std::make_tuple(dev, (const void*)kernel, threads, smem);
+    bool have = false;
+    {
+        std::lock_guard<std::mutex> g(c.m);
+        const auto it = c.occupancy.find(key);
+        const auto is = c.sms.find(dev);
+        if (it != c.occupancy.end() && is != c.sms.end()) {
+            per_sm = it->second;
+            sms = is->second;
+            have = true;
+        }
+    }
+    if (!have) {
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e != cudaSuccess) return e;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+        if (e != cudaSuccess) return e;
+        std::lock_guard<std::mutex> g(c.m);
+        c.occupancy[key] = per_sm;
+        c.sms[dev] = sms;
+    }
     blocks = (long)(per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
     if (cap > 0 && blocks > cap) blocks = cap;
     if (blocks > tasks) blocks = tasks > 0 ? tasks : 1;
@@ -1954,11 +1997,13 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
         if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31, false>;
         if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41, false>;
         const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, false);
-        e = allow_max_smem(fast);
-        if (e != cudaSuccess) return e;
-        e = one_wave(fast, FL.bytes, 0, a.n_tasks, blocks);
-        if (e != cudaSuccess) return e;
-        fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
+        if (!a.rescue_all) {
+            e = allow_max_smem(fast);
+            if (e != cudaSuccess) return e;
+            e = one_wave(fast, FL.bytes, 0, a.n_tasks, blocks);
+            if (e != cudaSuccess) return e;
+            fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
+        }
         // the rescue pass: a block of kCoopWarps warps per task
         const StagedLayout RL = staged_layout(a.n, a.tile_w, a.tile_h, true, true);
         e = allow_max_smem(coop_rescue_kernel<SIX>);
@@ -2042,6 +2087,15 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     const StagedLayout SL = staged_layout(a.n, tw, th);
     const bool staged_ok = ((a.n + 31) >> 5) <= kFastMaxPerLane && SL.bytes <= kFastMaxSmem;
     a.general_all = staged_ok ? 0 : 1;
+    // A launch of a few tasks per SM (Path B rounds, the anchor lattice, patch
+    // solves) is bound by each task's latency: every task then goes to the
+    // rescue pass, whose 8 warps per task sample each evaluation together.
+    // Both passes give the same result for a task.
+    int sms = 0, dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+        a.rescue_all = staged_ok && a.n_tasks <= 4 * sms ? 1 : 0;
+    else
+        a.rescue_all = 0;
     // reference planes of another frame are read by the staged solver only
     const bool own_ref = (a.ref_pitch > 0 && a.ref_pitch != a.pitch) || a.ref_dx != 0 || a.ref_dy != 0;
     if (own_ref && !staged_ok) return cudaErrorInvalidValue;

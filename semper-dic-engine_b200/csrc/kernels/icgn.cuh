@@ -37,6 +37,7 @@ struct SolveArgs {
     int half, n, min_valid;
     int off_tile, off_vals, off_valid, off_refok;
     int general_all;  // set by launch_solve: the general pass takes every task (no fast pass)
+    int rescue_all;   // set by launch_solve: the rescue pass takes every task (small launches)
     // Reference planes other than the deformed image's frame: the subset
     // centred at (cx, cy) is read at (cx + ref_dx, cy + ref_dy) of planes with
     // row pitch ref_pitch (0: the same planes frame, pitch). Staged solver only.
