@@ -803,9 +803,10 @@ struct StagedLayout {
 // the block samples a share of the subset for each evaluation.
 constexpr int kCoopWarps = 8;
 struct CoopReq {
-    int op;  // 0: done, 1: sample, 2: coarse search
+    int op;  // 0: done, 1: sample, 2: coarse search, 3: stage the reference subset
     int cx, cy, tile_ok, tx0, ty0;
     float Wp[6];
+    float mref, iref;
 };
 constexpr int kCoopBytes = 64 + kCoopWarps * 32 * 8 + kCoopWarps * 8;
 
@@ -926,11 +927,39 @@ struct WarpSolver {
             Hr[k] = Hs21[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
         }
         ref_base = (cy - half + ref_dy) * ref_pitch + (cx - half + ref_dx);
-        refok = 0;
+        if constexpr (COOP) {
+            // every warp of the block stages a share of the subset
+            const int per = (K + kCoopWarps - 1) / kCoopWarps;
+            coop_post(3, nullptr);
+            int g = 0;
+            Mask bits = stage_part(0, min(K, per), g);
+            g = wsum(g);
+            coop_bar();
+#pragma unroll
+            for (int w = 1; w < kCoopWarps; ++w) {
+                bits |= gbits[w * 32 + lane];
+                g += (int)cslots[w].x;
+            }
+            refok = bits;
+            ghost = g;
+            __syncwarp();
+            return;
+        }
         int g = 0;
-        int row = row0, col = col0;
+        refok = stage_part(0, K, g);
+        ghost = wsum(g);
+        __syncwarp();
+    }
+
+    // The reference pixels k in [k_lo, k_hi) of this lane: their non-Ghost
+    // bits returned, their Ghost count added to g, and (STAGE) the subset
+    // staged normalised with its raw gradients.
+    __device__ __forceinline__ Mask stage_part(int k_lo, int k_hi, int& g) {
+        Mask bits = 0;
+        const int i0 = lane + 32 * k_lo;
+        int row = i0 / dim, col = i0 - (i0 / dim) * dim;
 #pragma unroll 4
-        for (int k = 0; k < K; ++k) {
+        for (int k = k_lo; k < k_hi; ++k) {
             const int i = lane + 32 * k;
             if (i < n) {
                 const int idx = ref_base + row * ref_pitch + col;
@@ -938,7 +967,7 @@ struct WarpSolver {
                 if (I < kGhost)
                     ++g;
                 else
-                    refok |= Mask(1) << k;
+                    bits |= Mask(1) << k;
                 if constexpr (STAGE) {
                     srn[i] = (I - mref) * iref;
                     sgx[i] = __ldg(refGx + idx);
@@ -947,8 +976,7 @@ struct WarpSolver {
             }
             advance(row, col);
         }
-        ghost = wsum(g);
-        __syncwarp();
+        return bits;
     }
 
     // The tile must cover every sample support of the warped subset: stage a
@@ -1065,7 +1093,15 @@ struct WarpSolver {
             lo_y = (float)(4 - cy);
             hi_y = (float)(H - 4 - cy);
             ref_base = (cy - half + ref_dy) * ref_pitch + (cx - half + ref_dx);
-            if (op == 1) {
+            if (op == 3) {
+                mref = req->mref;
+                iref = req->iref;
+                const int lo = warp * per, hi = min(K, lo + per);
+                int g = 0;
+                gbits[warp * 32 + lane] = lo < hi ? stage_part(lo, hi, g) : Mask(0);
+                g = wsum(g);
+                if (lane == 0) cslots[warp] = make_float2((float)g, 0.0f);
+            } else if (op == 1) {
                 tile_ok = req->tile_ok != 0;
                 tx0 = req->tx0;
                 ty0 = req->ty0;
@@ -1090,6 +1126,8 @@ struct WarpSolver {
             req->tile_ok = tile_ok ? 1 : 0;
             req->tx0 = tx0;
             req->ty0 = ty0;
+            req->mref = mref;
+            req->iref = iref;
             if (Wp)
                 for (int k = 0; k < 6; ++k) req->Wp[k] = Wp[k];
         }
