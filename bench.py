@@ -496,7 +496,7 @@ def main():
                          "settings), cfg4-large (large deformation seeded by the global-motion estimate), cfg3 "
                          "(incremental sample)")
     ap.add_argument("--pairs", type=int, default=256, help="cfg2: pairs per batch")
-    ap.add_argument("--workers", type=int, default=4, help="cfg2: concurrent engines")
+    ap.add_argument("--workers", type=int, default=8, help="cfg2: concurrent engines")
     ap.add_argument("--interval", type=int, default=1, help="cfg3: the session's update_interval")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -85,7 +85,7 @@ typedef struct semper_b200_job {
 
 typedef struct semper_b200_batch semper_b200_batch;
 
-/* A batch runner with `workers` engines (<= 0: 4), each with its own stream
+/* A batch runner with `workers` engines (<= 0: 8), each with its own stream
    and host thread, on the current device. NULL on failure. */
 SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers);
 SEMPER_C_API void semper_b200_batch_destroy(semper_b200_batch* b);

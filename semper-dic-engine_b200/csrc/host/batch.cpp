@@ -68,7 +68,7 @@ extern "C" {
 
 SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers) {
     try {
-        if (workers <= 0) workers = 4;
+        if (workers <= 0) workers = 8;
         auto* b = new semper_b200_batch();
         if (cudaGetDevice(&b->device) != cudaSuccess) {
             delete b;

@@ -230,7 +230,7 @@ class Engine:
 class Batch:
     """semper_b200_batch: independent pairs solved concurrently."""
 
-    def __init__(self, workers: int = 4):
+    def __init__(self, workers: int = 8):
         self._h = lib().semper_b200_batch_create(workers)
         if not self._h:
             raise RuntimeError("semper_b200_batch_create failed")
