@@ -15,6 +15,19 @@ namespace dic {
 
 namespace {
 
+// x / 12 correctly rounded for an integer-valued x with |x| <= 2295 (the
+// gradient numerators of 8-bit images): the quotient by the rounded
+// reciprocal, then one FMA residual correction (Markstein's method for a
+// divisor known in advance). For these numerators the result equals the IEEE
+// quotient bit for bit; the tests compare the planes with the CPU
+// restatement's divisions.
+__device__ __forceinline__ float div12(float x) {
+    const float inv = 1.0f / 12.0f;  // RN(1/12), folded at compile time
+    const float q = x * inv;
+    const float r = __fmaf_rn(-q, 12.0f, x);
+    return __fmaf_rn(r, inv, q);
+}
+
 // One thread per 4 horizontally adjacent pixels: u8 -> f32 intensity and the
 // 4th-order central-difference gradients (zero within 2 px of the border),
 // then the Ghost Wall where the mask is below 128. Integer numerators make
@@ -29,8 +42,44 @@ __global__ void image_kernel(const uint8_t* __restrict__ px, const uint8_t* __re
     const size_t row = (size_t)y * W;
     const size_t orow = (size_t)y * pitch;
     float vi[4], vx[4], vy[4];
+    // Interior threads of 4-byte-aligned rows read their bytes as words: three
+    // of the row (x0 - 4 .. x0 + 7) and one of each of the four rows above and
+    // below; the same integer numerators as the byte path.
+    const bool words = ((W & 3) == 0) && ((reinterpret_cast<uintptr_t>(px) & 3) == 0) && x0 >= 4 && x0 + 8 <= W &&
+                       y >= 2 && y < H - 2;
+    if (words) {
+        const uint32_t* r = reinterpret_cast<const uint32_t*>(px + row) + (x0 >> 2);
+        const size_t wr = (size_t)W >> 2;
+        const uint32_t a = __ldg(r - 1), b = __ldg(r), c = __ldg(r + 1);
+        const uint32_t u1 = __ldg(r - wr), u2 = __ldg(r - 2 * wr), d1 = __ldg(r + wr), d2 = __ldg(r + 2 * wr);
+        int v[12];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < 4; ++k) {
+            v[k] = (int)((a >> (8 * k)) & 0xffu);
+            v[4 + k] = (int)((b >> (8 * k)) & 0xffu);
+            v[8 + k] = (int)((c >> (8 * k)) & 0xffu);
+        }
+        uint32_t m = 0xffffffffu;
+        if (mask) {
+            if ((reinterpret_cast<uintptr_t>(mask) & 3) == 0)
+                m = __ldg(reinterpret_cast<const uint32_t*>(mask + row) + (x0 >> 2));
+            else
+                m = (uint32_t)__ldg(mask + row + x0) | ((uint32_t)__ldg(mask + row + x0 + 1) << 8) |
+                    ((uint32_t)__ldg(mask + row + x0 + 2) << 16) | ((uint32_t)__ldg(mask + row + x0 + 3) << 24);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int nx = -v[6 + k] + 8 * v[5 + k] - 8 * v[3 + k] + v[2 + k];
+            const int ny = -(int)((d2 >> (8 * k)) & 0xffu) + 8 * (int)((d1 >> (8 * k)) & 0xffu) -
+                           8 * (int)((u1 >> (8 * k)) & 0xffu) + (int)((u2 >> (8 * k)) & 0xffu);
+            vi[k] = (float)v[4 + k];
+            vx[k] = div12((float)nx);
+            vy[k] = div12((float)ny);
+            if (((m >> (8 * k)) & 0xffu) < 128u) vi[k] = -10.0f;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4 && !words; ++k) {
         const int x = x0 + k;
         vi[k] = vx[k] = vy[k] = 0.0f;
         if (x >= W) continue;
@@ -41,8 +90,8 @@ __global__ void image_kernel(const uint8_t* __restrict__ px, const uint8_t* __re
                            (int)__ldg(px + p - 2);
             const int ny = -(int)__ldg(px + p + 2 * (size_t)W) + 8 * (int)__ldg(px + p + W) -
                            8 * (int)__ldg(px + p - W) + (int)__ldg(px + p - 2 * (size_t)W);
-            vx[k] = __fdiv_rn((float)nx, 12.0f);
-            vy[k] = __fdiv_rn((float)ny, 12.0f);
+            vx[k] = div12((float)nx);
+            vy[k] = div12((float)ny);
         }
         if (mask && __ldg(mask + p) < 128) vi[k] = -10.0f;
     }
