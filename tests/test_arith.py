@@ -4,9 +4,9 @@ The image preparation divides each gradient numerator by 12 as the quotient
 by the rounded reciprocal plus one FMA correction (prep.cu, div12) instead of
 an IEEE division. For this to leave the planes bit-identical to the CPU
 restatement (which divides), the two must agree for every numerator an 8-bit
-image can produce: -255 - 8*0 ... i.e. |x| <= 9 * 255 = 2295. Checked here
-with exact rational arithmetic and correct float32 rounding, no FMA emulation
-shortcuts.
+image can produce: -I[x+2] + 8 I[x+1] - 8 I[x-1] + I[x-2] lies within
+|x| <= 9 * 255 = 2295. Checked here with exact rational arithmetic and correct
+float32 rounding.
 """
 from fractions import Fraction
 
