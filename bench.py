@@ -162,6 +162,39 @@ def cpu_sample(ref, dfm, prm, fp64=False, model=None):
     return rc, dt, int(met[0]), pts, p
 
 
+def accuracy_sample(eng, ref, dfm, prm, warp, p, gm):
+    """The device's field on the CPU sample's ROI against the same solve in
+    FP64 (the CPU restatement in double, given the same global model) and
+    against the synthetic warp's true displacement; after the timed region."""
+    import semper_b200 as sb
+
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+
+    roi = sb.params((p[0], p[1], p[2], p[3]), p[4], p[5], p[6], six=bool(p[7]))
+    model = gm["H"] if gm["locked"] else None
+    eng.set_global_model(model)  # both solves seeded from the same model
+    rc, pts, _ = eng.run(dfm, roi)
+    eng.set_global_model(None)
+    o = oracle.Oracle(True)
+    o.set_reference(ref)
+    orc, opts, _ = o.run(dfm, p, model_h=model)
+    if rc <= 0 or orc <= 0:
+        return {"note": f"no points to compare (device {rc}, FP64 {orc})"}
+    key = {(float(x), float(y)): i for i, (x, y) in enumerate(opts[:, :2])}
+    both = [(i, key[(float(x), float(y))]) for i, (x, y) in enumerate(pts[:, :2]) if (float(x), float(y)) in key]
+    a = np.array([pts[i] for i, _ in both])
+    b = np.array([opts[j] for _, j in both])
+    d = np.abs(a[:, 2:4] - b[:, 2:4])
+    u, v = sb.displacement(warp, pts[:, 0], pts[:, 1])
+    t = np.hypot(pts[:, 2] - u, pts[:, 3] - v)
+    return {"roi": [p[0], p[1], p[2], p[3]], "points_device": int(rc), "points_fp64": int(orc),
+            "points_compared": len(both),
+            "vs_fp64_max_px": float(d.max()), "vs_fp64_rms_px": float(np.sqrt(np.mean(d ** 2))),
+            "vs_fp64_strain_max": float(np.abs(a[:, 4:7] - b[:, 4:7]).max()),
+            "vs_true_field_rms_px": float(np.sqrt(np.mean(t ** 2))), "vs_true_field_max_px": float(t.max())}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return 0
@@ -309,11 +342,13 @@ def run_b200(args, rank, world, local_rank):
     line = None
     if rank == 0:
         cpu = None
+        accuracy = None
         if world == 1 and not args.no_cpu:
             crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm, model=gm["H"] if gm["locked"] else None)
             cpu = {"value": crc / cdt, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
                    "sample": f"central {cp[2]}x{cp[3]} ROI ({cp[2] // cp[4]}^2 grid, {catt} attempted) of the "
                              f"same pair, reference cache warm, {cdt:.2f} s"}
+            accuracy = accuracy_sample(eng, ref, dfm, prm, warp, cp, gm)
         mean_phase = {k: round(statistics.mean(p[k] for p in phases), 3) for k in phases[0]}
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
@@ -347,6 +382,8 @@ def run_b200(args, rank, world, local_rank):
         }
         if cpu:
             line["cpu_baseline"] = cpu
+        if accuracy:
+            line["accuracy"] = accuracy
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
