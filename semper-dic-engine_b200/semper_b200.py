@@ -163,9 +163,10 @@ class Engine:
             raise RuntimeError("semper_create failed (no usable CUDA device?)")
 
     def close(self):
-        if getattr(self, "_h", None):
-            lib().semper_destroy(self._h)
-            self._h = None
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h and _lib is not None:  # at interpreter exit the library may be gone already
+            _lib.semper_destroy(h)
 
     __del__ = close
 
@@ -236,9 +237,10 @@ class Batch:
             raise RuntimeError("semper_b200_batch_create failed")
 
     def close(self):
-        if getattr(self, "_h", None):
-            lib().semper_b200_batch_destroy(self._h)
-            self._h = None
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h and _lib is not None:  # at interpreter exit the library may be gone already
+            _lib.semper_b200_batch_destroy(h)
 
     __del__ = close
 
@@ -328,9 +330,10 @@ class Incremental:
             raise RuntimeError("semper_incremental_create failed")
 
     def close(self):
-        if getattr(self, "_h", None):
-            lib().semper_incremental_destroy(self._h)
-            self._h = None
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h and _lib is not None:  # at interpreter exit the library may be gone already
+            _lib.semper_incremental_destroy(h)
 
     __del__ = close
 
