@@ -20,6 +20,7 @@
 #include <cmath>
 #include <condition_variable>
 #include <cstring>
+#include <map>
 #include <deque>
 #include <mutex>
 #include <queue>
@@ -333,6 +334,27 @@ struct Engine::Impl {
     }
     void poll_cancel() {
         if (E.h_cancel_[0]) throw Cancelled{};
+    }
+
+    // Autotuner of the fast pass's shape, per (subset size, interpolator): the
+    // first large Path A launch reads the reference subset from the planes,
+    // the second stages it in shared memory; the faster per subset
+    // pixel-iteration is kept from then on. Both shapes give the same results,
+    // so the choice changes the time only.
+    struct Tune {
+        int trials = 0, best = -1;
+        double t[2] = {0.0, 0.0};
+    };
+    std::map<std::pair<int, int>, Tune> tune;
+    int tune_pick(int dim, int six) {
+        const Tune& t = tune[{dim, six}];
+        return t.best >= 0 ? t.best : t.trials % 2;
+    }
+    void tune_record(int dim, int six, int variant, double ms_per_pixel_iter) {
+        Tune& t = tune[{dim, six}];
+        if (t.best >= 0 || !(ms_per_pixel_iter > 0.0)) return;
+        t.t[variant] = ms_per_pixel_iter;
+        if (++t.trials >= 2) t.best = t.t[1] < t.t[0] ? 1 : 0;
     }
 
     dic::SolveArgs solve_args(int dim, int six) {
@@ -1127,6 +1149,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
 
         // ---------------------------------------------------------------- Path A
         const auto t_a = clk::now();
+        int tune_variant = 0;
         tasks.ensure(std::max(tasks.n, NG));
         results.ensure(std::max(results.n, NG));
         deferred.ensure(std::max(deferred.n, NG));
@@ -1143,6 +1166,8 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             a.tasks = tasks.p;
             a.n_tasks_dev = counters.p + 1;
             a.n_tasks = n_a;
+            tune_variant = tune_pick(dim, params.six ? 1 : 0);
+            a.fast_stage = tune_variant;
             a.results = results.p;
             a.deferred = deferred.p;
             check(cudaEventRecord(ev[5], st), "event");
@@ -1158,6 +1183,9 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             float ms = 0.f;
             check(cudaEventElapsedTime(&ms, ev[5], ev[6]), "elapsed");
             E.times_.path_a = ms;
+            // launches small enough to go straight to the rescue pass run no fast pass
+            if (n_a > 4 * sm_count && ps.icgn_iters > 0)
+                tune_record(dim, params.six ? 1 : 0, tune_variant, ms / ((double)dim * dim * ps.icgn_iters));
         }
         E.times_.path_a_tasks = n_a;
         st_a.icgn_iters = (long long)ps.icgn_iters;

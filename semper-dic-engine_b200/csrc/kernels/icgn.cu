@@ -2027,14 +2027,15 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
         int tw = 0, th = 0;
         tile_box(a.dim, SIX ? 1 : 0, tw, th);
         const bool box_ok = a.tile_w == 0 || (a.tile_w == tw && a.tile_h == th);
-        // the fast pass reads the reference subset from the planes (through
-        // L1): without the staged copy a warp needs about half the shared
-        // memory, and twice as many warps fit an SM
-        auto fast = fast_kernel<SIX, 0, false>;
-        if (box_ok && a.dim == 21) fast = fast_kernel<SIX, 21, false>;
-        if (box_ok && a.dim == 31) fast = fast_kernel<SIX, 31, false>;
-        if (box_ok && a.dim == 41) fast = fast_kernel<SIX, 41, false>;
-        const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, false);
+        // the fast pass reads the reference subset from the planes (about
+        // half the shared memory per warp, twice the resident warps) or
+        // stages it per task (fast_stage): the caller's autotuner times both
+        const bool stage = a.fast_stage != 0;
+        auto fast = stage ? fast_kernel<SIX, 0, true> : fast_kernel<SIX, 0, false>;
+        if (box_ok && a.dim == 21) fast = stage ? fast_kernel<SIX, 21, true> : fast_kernel<SIX, 21, false>;
+        if (box_ok && a.dim == 31) fast = stage ? fast_kernel<SIX, 31, true> : fast_kernel<SIX, 31, false>;
+        if (box_ok && a.dim == 41) fast = stage ? fast_kernel<SIX, 41, true> : fast_kernel<SIX, 41, false>;
+        const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, stage);
         if (!a.rescue_all) {
             e = allow_max_smem(fast);
             if (e != cudaSuccess) return e;
