@@ -1343,7 +1343,11 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 return true;
             };
             // Round k runs on slot k % 2; its solves start as soon as it is
-            // claimed, so two rounds run on the device at once.
+            // claimed, so two rounds run on the device at once. A slot's host
+            // buffers are rewritten only once its previous work is done (an
+            // earlier run that ended early may have left some queued).
+            for (const Slot& S : slots)
+                if (S.s) check(cudaStreamSynchronize(S.s), "slot drain");
             check(cudaEventRecord(ev[9], st), "event");
             int launched_rounds = 0, done_rounds = 0;
             auto claim_launch = [&]() -> bool {
@@ -1455,7 +1459,11 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         }
         return valid_count;
     } catch (const Cancelled&) {
+        // work still queued (Path B rounds on their slot streams included) ends
+        // before the next run reuses the buffers it reads and writes
         cudaStreamSynchronize(st);
+        for (const Slot& S : slots)
+            if (S.s) cudaStreamSynchronize(S.s);
         return -99;
     }
 }

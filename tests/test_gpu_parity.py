@@ -257,3 +257,43 @@ def test_autotuned_fast_pass_shapes_agree():
     for rc, pts, met in runs[1:]:
         assert rc == runs[0][0] and np.array_equal(pts, runs[0][1])
         assert np.array_equal(met[COUNT_SLOTS], runs[0][2][COUNT_SLOTS])
+
+
+def test_run_device_equals_run():
+    """semper_b200_run_device (frame and output in device memory) gives the
+    points semper_run gives for the same frame."""
+    import torch
+
+    ref, dfm, prm, _ = sb.config_pair(0, size=384)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    rc, pts, met = e.run(dfm, prm)
+    cap = (prm.rect_w // prm.step) * (prm.rect_h // prm.step) * 8
+    d_def = torch.from_numpy(dfm).cuda()
+    d_out = torch.zeros(cap, dtype=torch.float32, device="cuda")
+    rc2, met2 = e.run_device(d_def, prm, d_out, cap)
+    torch.cuda.synchronize()
+    assert rc2 == rc > 0
+    assert np.array_equal(d_out[: rc * 8].cpu().numpy().reshape(-1, 8), pts)
+    assert np.array_equal(met2[COUNT_SLOTS], met[COUNT_SLOTS])
+
+
+def test_cancel_during_run():
+    """semper_cancel from inside the run (the progress callback) ends it with
+    SEMPER_ERR_CANCELLED; the next run on the handle is unaffected."""
+    ref, dfm, prm, _ = sb.config_pair(0, size=384)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    seen = []
+
+    def cb(pct, user):
+        seen.append(pct)
+        e.cancel()
+
+    rc, _, _ = e.run(dfm, prm, progress=cb)
+    assert seen and rc == sb.SEMPER_ERR_CANCELLED
+    rc2, pts, _ = e.run(dfm, prm)
+    assert rc2 > 0
+    e.cancel()  # a cancel between runs does not carry over to the next run
+    rc3, pts3, _ = e.run(dfm, prm)
+    assert rc3 == rc2 and np.array_equal(pts3, pts)
