@@ -164,7 +164,15 @@ int IncrementalSession::process(const uint8_t* def, float* out, int capacity, fl
     semper_inc::FrameInfo fi;
     impl_->backend.prof = FrameProfile{};
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = impl_->core.process(def, out, capacity, metrics, metrics_len, progress, &fi);
+    int rc;
+    try {
+        rc = impl_->core.process(def, out, capacity, metrics, metrics_len, progress, &fi);
+    } catch (...) {
+        // a cancel seen by a solve outside the frame's full-field run (an
+        // anchor match) ends the frame the same way
+        if (!impl_->engine.cancel_requested()) throw;
+        rc = -99;
+    }
     impl_->backend.prof.total = ms_since(t0);
     if (info) {
         info->reference_frame = fi.reference_frame;

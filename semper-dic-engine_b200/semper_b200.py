@@ -344,14 +344,18 @@ class Incremental:
                                              0 if m is None else m.size, g.shape[1], g.shape[0],
                                              ctypes.byref(prm), update_interval)
 
-    def process(self, frame, capacity: int, metrics_len: int = 24):
+    def process(self, frame, capacity: int, metrics_len: int = 24, progress=None):
         d = np.ascontiguousarray(frame, np.uint8)
         out = np.zeros(max(capacity, 1), np.float32)
         met = np.zeros(max(metrics_len, 1), np.float32)
         info = IncrementalInfo()
+        cb = PROGRESS_CB(progress) if progress else PROGRESS_CB()
         rc = lib().semper_incremental_process(self._h, _p(d, _u8p), d.size, _p(out, _f32p), capacity,
-                                              _p(met, _f32p), metrics_len, ctypes.byref(info), PROGRESS_CB(), None)
+                                              _p(met, _f32p), metrics_len, ctypes.byref(info), cb, None)
         return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info
+
+    def cancel(self):
+        lib().semper_incremental_cancel(self._h)
 
     def profile(self) -> dict:
         """Where the last process() call spent its time (semper_b200_incremental_profile)."""

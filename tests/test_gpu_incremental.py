@@ -105,3 +105,23 @@ def test_first_frame_is_a_fixed_reference_run():
     rc2, pts2, _m2 = e.run(frames[0], prm)
     assert rc == rc2 and np.array_equal(pts, pts2)
     assert info.reference_updated == 1 and info.frame0_points == 625
+
+
+def test_cancel_during_frame():
+    """semper_incremental_cancel from inside a frame ends it with
+    SEMPER_ERR_CANCELLED and leaves the session as it was: the frame processed
+    again gives what an uncancelled session gives. The pair is one whose solve
+    runs through thousands of Path B rounds (a masked 1745^2 frame at subset
+    31, step 4), so the cancel, raised by the progress callback when seeding
+    starts, is seen by a later round."""
+    j = sb.batch_jobs(3, seed=0)[2]
+    prm = j["prm"]
+    cap = (prm.rect_w // prm.step) * (prm.rect_h // prm.step) * 8
+    a, b = sb.Incremental(), sb.Incremental()
+    assert a.init(j["ref"], prm, 1, mask=j["mask"]) == 0 and b.init(j["ref"], prm, 1, mask=j["mask"]) == 0
+    rc, _, _, _ = a.process(j["dfm"], cap, progress=lambda pct, user: a.cancel())
+    assert rc == sb.SEMPER_ERR_CANCELLED
+    ra, pa, _, ia = a.process(j["dfm"], cap)
+    rb, pb, _, ib = b.process(j["dfm"], cap)
+    assert ra == rb > 0 and np.array_equal(pa, pb)
+    assert ia.reference_frame == ib.reference_frame

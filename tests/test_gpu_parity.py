@@ -278,22 +278,32 @@ def test_run_device_equals_run():
     assert np.array_equal(met2[COUNT_SLOTS], met[COUNT_SLOTS])
 
 
+def _long_pair():
+    """A pair whose lattice does not reach full quality (a masked 1745^2 frame
+    at subset 31, step 4): Path B's rounds take it, some 4,000 of them, so a
+    solve lasts hundreds of milliseconds and polls the cancel flag in every
+    round."""
+    return sb.batch_jobs(3, seed=0)[2]
+
+
 def test_cancel_during_run():
-    """semper_cancel from inside the run (the progress callback) ends it with
-    SEMPER_ERR_CANCELLED; the next run on the handle is unaffected."""
-    ref, dfm, prm, _ = sb.config_pair(0, size=384)
+    """semper_cancel from inside the run (the progress callback, which the
+    engine's ticker thread calls as soon as seeding starts) ends it with
+    SEMPER_ERR_CANCELLED; the next run on the handle is unaffected, and a
+    cancel between runs does not carry over."""
+    j = _long_pair()
     e = sb.Engine()
-    assert e.set_reference(ref) == 0
+    assert e.set_reference(j["ref"], j["mask"]) == 0
     seen = []
 
     def cb(pct, user):
         seen.append(pct)
         e.cancel()
 
-    rc, _, _ = e.run(dfm, prm, progress=cb)
+    rc, _, _ = e.run(j["dfm"], j["prm"], mask=j["mask"], progress=cb)
     assert seen and rc == sb.SEMPER_ERR_CANCELLED
-    rc2, pts, _ = e.run(dfm, prm)
+    rc2, pts, _ = e.run(j["dfm"], j["prm"], mask=j["mask"])
     assert rc2 > 0
-    e.cancel()  # a cancel between runs does not carry over to the next run
-    rc3, pts3, _ = e.run(dfm, prm)
+    e.cancel()
+    rc3, pts3, _ = e.run(j["dfm"], j["prm"], mask=j["mask"])
     assert rc3 == rc2 and np.array_equal(pts3, pts)
