@@ -211,6 +211,7 @@ struct Engine::Impl {
     DevBuf<uint8_t> dGray;           // deformed frame bytes
     DevBuf<uint8_t> rGray;           // reference frame bytes (global motion)
     bool ref_gray = false;           // rGray holds the current reference
+    bool ref_ghost = false;          // the reference planes may hold Ghost Wall pixels (a mask was given)
     const uint8_t* last_def = nullptr;
     dic::GlobalMotion gm;
     DevBuf<float> dI, dGx, dGy;      // deformed planes (gradients kept for adoption)
@@ -375,6 +376,7 @@ struct Engine::Impl {
         a.lm = 1;
         a.cancel = E.d_cancel_;
         a.queue = solve_q.p;
+        a.ref_no_ghost = ref_ghost ? 0 : 1;
         (void)six;
         return a;
     }
@@ -505,6 +507,7 @@ void Engine::reset() {
     W_ = H_ = 0;
     impl_->grid_valid = false;
     impl_->ref_gray = false;
+    impl_->ref_ghost = false;
     impl_->last_def = nullptr;
     last_global_ = dic::GlobalSimilarity();
 }
@@ -533,6 +536,7 @@ int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask
     std::swap(I.rGray.p, I.dGray.p);  // the reference bytes stay for the global motion estimate
     std::swap(I.rGray.n, I.dGray.n);
     I.ref_gray = true;
+    I.ref_ghost = mask != nullptr;
     W_ = w;
     H_ = h;
     has_ref_ = true;
@@ -556,6 +560,7 @@ int Engine::adopt_last_deformed(const uint8_t* mask) {
         std::swap(I.rGray.n, I.dGray.n);
     }
     I.last_def = nullptr;
+    I.ref_ghost = mask != nullptr;
     if (mask) {
         // Ghost Wall on the adopted frame: the gradients stay those of the
         // real intensities (stamp after prepare, reference_cache.cpp:95-96).
@@ -682,6 +687,7 @@ PatchSolve Engine::solve_patch(const uint8_t* patch, int size, int ax, int ay, f
     t.g[1] = gv;
     check(cudaMemcpyAsync(I.aTask.p, &t, sizeof(t), cudaMemcpyHostToDevice, st), "H2D patch task");
     dic::SolveArgs a = I.solve_args(subset, six ? 1 : 0);
+    a.ref_no_ghost = 0;  // the patch planes, not the reference's
     a.refI = I.aI.p;
     a.refGx = I.aGx.p;
     a.refGy = I.aGy.p;

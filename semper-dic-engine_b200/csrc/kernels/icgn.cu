@@ -868,6 +868,7 @@ struct WarpSolver {
     // ensure_tile
     bool all_in;
     Mask fullmask;  // bit k set when pixel lane + 32 k exists
+    bool no_ghost;  // no reference pixel is a Ghost Wall pixel (launch constant)
     unsigned phase;
     // the task
     int cx, cy, ref_base, ghost;
@@ -944,6 +945,14 @@ struct WarpSolver {
             ghost = g;
             __syncwarp();
             return;
+        }
+        if constexpr (!STAGE) {
+            if (no_ghost) {
+                // nothing to stage and nothing to count: every pixel is valid reference
+                refok = fullmask;
+                ghost = 0;
+                return;
+            }
         }
         int g = 0;
         refok = stage_part(0, K, g);
@@ -1760,6 +1769,7 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
     s.tile_ok = false;
     s.tile_on = tw > 0;
     s.all_in = false;
+    s.no_ghost = false;
     s.fullmask = 0;
     for (int k = 0; k < s.K; ++k)
         if (lane + 32 * k < n) s.fullmask |= Mask(1) << k;
@@ -1790,6 +1800,7 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
                  DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
                  a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
     if (DIMC > 0) s.tile_on = a.tile_w > 0;
+    s.no_ghost = a.ref_no_ghost != 0;
     const int lane = s.lane, dim = s.dim, half = s.half;
     const int ntasks = a.n_tasks_dev ? *a.n_tasks_dev : a.n_tasks;
     int* const n_deferred = a.queue + 2;

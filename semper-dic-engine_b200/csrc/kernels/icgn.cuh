@@ -38,6 +38,8 @@ struct SolveArgs {
     int off_tile, off_vals, off_valid, off_refok;
     int general_all;  // set by launch_solve: the general pass takes every task (no fast pass)
     int rescue_all;   // set by launch_solve: the rescue pass takes every task (small launches)
+    int ref_no_ghost; // the caller's promise: no reference pixel is below the Ghost Wall threshold
+                      // (no mask), so the fast pass skips its per-task scan for them
     int fast_stage;   // the caller's choice: the fast pass stages the reference subset (1) or reads
                       // the planes (0); the same results either way
     // Reference planes other than the deformed image's frame: the subset
