@@ -1337,8 +1337,14 @@ struct WarpSolver {
             const float inv = 1.0f / sdev;
 
             float ep = 0.0f, gp0 = 0.0f, gp1 = 0.0f, gp2 = 0.0f, gp3 = 0.0f, gp4 = 0.0f, gp5 = 0.0f;
+            // the texture check's sums of the raw gradients over the same valid
+            // pixels in the same order, taken here where the gradients are
+            // loaded anyway (reference read from the planes)
+            float tsx = 0.0f, tsy = 0.0f;
             // one pixel's share of the residual and the steepest-descent sums
             auto accumulate = [&](int i, float I, float gx, float gy, float fx, float fy) {
+                tsx = __fmaf_rn(gx, gx, tsx);
+                tsy = __fmaf_rn(gy, gy, tsy);
                 const float rn = (I - mref) * iref, g0 = gx * iref, g1 = gy * iref;
                 const float nd = (vals[i] - mean) * inv;
                 const float diff = rn - nd;
@@ -1464,16 +1470,21 @@ struct WarpSolver {
             if (sqrtf(nn) < 0.001f) {
                 // texture check on the raw reference gradients (optimization_engine.cpp:435-461)
                 float sx = 0.0f, sy = 0.0f;
-                int row = row0, col = col0;
+                if constexpr (STAGE) {
+                    int row = row0, col = col0;
 #pragma unroll 4
-                for (int k = 0; k < K; ++k) {
-                    if ((valid >> k) & 1u) {
-                        const int i = lane + 32 * k;
-                        const float gx = gx_at(i, row, col), gy = gy_at(i, row, col);
-                        sx = __fmaf_rn(gx, gx, sx);
-                        sy = __fmaf_rn(gy, gy, sy);
+                    for (int k = 0; k < K; ++k) {
+                        if ((valid >> k) & 1u) {
+                            const int i = lane + 32 * k;
+                            const float gx = sgx[i], gy = sgy[i];
+                            sx = __fmaf_rn(gx, gx, sx);
+                            sy = __fmaf_rn(gy, gy, sy);
+                        }
+                        advance(row, col);
                     }
-                    advance(row, col);
+                } else {
+                    sx = tsx;  // this iteration's residual pass summed them
+                    sy = tsy;
                 }
                 const float tx = wsum(sx), ty = wsum(sy);
                 const float sg = ty < tx ? ty : tx;
