@@ -1817,15 +1817,33 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
     int* const n_deferred = a.queue + 2;
     int* const deferred = a.deferred;
     int polled = 0;
+    // One task of lookahead: the next task is claimed, and its record loaded
+    // (word i of the 10 by lane i: one register a lane) while the current one
+    // is solved. The record passes through shared memory where the
+    // masked-iteration matrix of the rescue pass would be (unused here).
+    static_assert(sizeof(dic_task) == 40, "task record of 10 words");
+    int* const tn_s = reinterpret_cast<int*>(smem + 352);
+    int tw = 0;
+    auto fetch_task = [&](int tt) {
+        if (tt < ntasks && lane < 10) tw = reinterpret_cast<const int*>(a.tasks + tt)[lane];
+    };
+    int t_next = 0;
+    if (lane == 0) t_next = atomicAdd(a.queue, 1);
+    t_next = __shfl_sync(kFull, t_next, 0);
+    fetch_task(t_next);
     for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(a.queue, 1);
-        t = __shfl_sync(kFull, t, 0);
+        const int t = t_next;
         if (t >= ntasks) break;
         // the cancel flag lives in host memory: a read crosses PCIe, so a warp
         // looks at it once every kCancelPollTasks tasks, not per task
         if (a.cancel && (++polled & (kCancelPollTasks - 1)) == 0 && *(volatile const int*)a.cancel) break;
-        const dic_task T = a.tasks[t];
+        __syncwarp();
+        if (lane < 10) tn_s[lane] = tw;
+        __syncwarp();
+        const dic_task T = *reinterpret_cast<const dic_task*>(tn_s);
+        if (lane == 0) t_next = atomicAdd(a.queue, 1);
+        t_next = __shfl_sync(kFull, t_next, 0);
+        fetch_task(t_next);
         if (T.mode == DIC_INIT_AUTO_SEARCH || s.K > kFastMaxPerLane) {
             if (lane == 0) deferred[atomicAdd(n_deferred, 1)] = t;
             __syncwarp();
