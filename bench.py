@@ -366,6 +366,8 @@ def run_b200(args, rank, world, local_rank):
             "first_frame_pool_ms": round(first_t["pool"], 3),
             "phases_ms": mean_phase,
             "mean_icgn_iters_per_point": float(met[8]),
+            "fast_pass_shape": {0: "reference from the planes", 1: "reference staged", -1: "undecided"}[
+                eng.fast_pass_shape(prm.subset_size, bool(prm.use_6x6_interpolator))],
             "global_model": {"locked": gm["locked"], "rotation_deg": float(np.degrees(gm["theta"])),
                              "scale": gm["scale"], "translation_px": [float(gm["t"][0]), float(gm["t"][1])]},
             "e2e": {"value": e2e_value, "unit": "points/s",

@@ -34,6 +34,13 @@ SEMPER_C_API void* semper_b200_stream(semper_engine* eng);
    launched]. Returns 0, or -3 for a NULL handle. */
 SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], long long counts[5]);
 
+/* The shape of the Path A fast pass the engine's autotuner kept for this
+   subset size and interpolator (six != 0: 6x6 Keys): 0 reads the reference
+   subset from the prepared planes, 1 stages it in shared memory, -1 while
+   undecided (the first four large Path A launches alternate between them).
+   Both shapes give the same results. Returns -3 for a NULL handle. */
+SEMPER_C_API int semper_b200_fast_pass_shape(semper_engine* eng, int subset_size, int six);
+
 /* Where the last semper_incremental_process call spent its time (host wall
    clock, ms): out[0] the whole call, [1] its full-field solves, [2] its
    anchor matches, [3] the material-mask warp, [4] the reference adoption,

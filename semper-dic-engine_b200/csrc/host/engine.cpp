@@ -338,10 +338,13 @@ struct Engine::Impl {
     }
 
     // Autotuner of the fast pass's shape, per (subset size, interpolator): the
-    // first large Path A launch reads the reference subset from the planes,
-    // the second stages it in shared memory; the faster per subset
-    // pixel-iteration is kept from then on. Both shapes give the same results,
-    // so the choice changes the time only.
+    // first four large Path A launches alternate between reading the
+    // reference subset from the planes and staging it in shared memory; the
+    // shape with the lower of its two times per subset pixel-iteration is kept
+    // from then on (two trials each, so that the first frame's cold caches do
+    // not decide). Both shapes give the same results, so the choice changes
+    // the time only.
+    static constexpr int kTuneTrials = 4;
     struct Tune {
         int trials = 0, best = -1;
         double t[2] = {0.0, 0.0};
@@ -354,8 +357,8 @@ struct Engine::Impl {
     void tune_record(int dim, int six, int variant, double ms_per_pixel_iter) {
         Tune& t = tune[{dim, six}];
         if (t.best >= 0 || !(ms_per_pixel_iter > 0.0)) return;
-        t.t[variant] = ms_per_pixel_iter;
-        if (++t.trials >= 2) t.best = t.t[1] < t.t[0] ? 1 : 0;
+        if (t.t[variant] == 0.0 || ms_per_pixel_iter < t.t[variant]) t.t[variant] = ms_per_pixel_iter;
+        if (++t.trials >= kTuneTrials) t.best = t.t[1] < t.t[0] ? 1 : 0;
     }
 
     dic::SolveArgs solve_args(int dim, int six) {
@@ -510,6 +513,11 @@ void Engine::reset() {
     impl_->ref_ghost = false;
     impl_->last_def = nullptr;
     last_global_ = dic::GlobalSimilarity();
+}
+
+int Engine::fast_pass_shape(int subset_size, bool six) const {
+    const auto it = impl_->tune.find({subset_size, six ? 1 : 0});
+    return it == impl_->tune.end() ? -1 : it->second.best;
 }
 
 int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask) {

@@ -167,6 +167,10 @@ public:
 
     cudaStream_t stream() const { return stream_; }
     const PhaseTimes& last_times() const { return times_; }
+    // The fast pass's shape the autotuner kept for (subset size, interpolator):
+    // 0 the reference read from the planes, 1 staged in shared memory, -1 not
+    // decided yet.
+    int fast_pass_shape(int subset_size, bool six) const;
     // Grid blocks of the persistent solve kernel (0: automatic).
     void set_solve_blocks(int b) { solve_blocks_ = b; }
 

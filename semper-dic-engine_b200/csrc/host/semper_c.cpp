@@ -228,6 +228,11 @@ SEMPER_C_API int semper_b200_last_timings(semper_engine* eng, float times[8], lo
     return 0;
 }
 
+SEMPER_C_API int semper_b200_fast_pass_shape(semper_engine* eng, int subset_size, int six) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    return eng->engine.fast_pass_shape(subset_size, six != 0);
+}
+
 SEMPER_C_API int semper_b200_incremental_profile(semper_incremental* inc, double out[16]) {
     if (inc == nullptr || out == nullptr) return SEMPER_ERR_INIT;
     const semper_b200::FrameProfile& f = inc->session->last_profile();

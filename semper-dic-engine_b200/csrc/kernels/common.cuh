@@ -269,6 +269,136 @@ static __device__ __noinline__ bool well_conditioned(const double H[6][6], int h
     return well_conditioned_r(h, half);
 }
 
+// Warp-collective forms of inverse6_r and well_conditioned_r, for a block
+// whose other warps wait on the result: every entry is formed by the same
+// operations in the same order as in the one-thread forms, so the results
+// agree bit for bit. The chain of one column (square root, divisions) is the
+// critical path instead of the whole factorisation. Matrices are 36 doubles,
+// row-major, in shared memory; every lane of the warp takes part.
+//
+// Cholesky with lane i < 6 holding row i of L, the triangular inverse with
+// lane c < 6 holding column c of L^-1, and the product L^-T L^-1 with lane
+// m < 21 forming upper-triangle entry m. scr: 72 doubles. Ai is written when
+// the factorisation succeeds (factored), as by inverse6.
+__device__ __forceinline__ bool inverse6_warp(const double* A, double* Ai, double* scr, bool& factored) {
+    const int lane = threadIdx.x & 31;
+    double* Ls = scr;       // L, row-major
+    double* Lis = scr + 36;  // L^-1, row-major
+    double Lr[6];
+#pragma unroll
+    for (int c = 0; c < 6; ++c) Lr[c] = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        double Lj[6];
+#pragma unroll
+        for (int k = 0; k < j; ++k) Lj[k] = __shfl_sync(kFull, Lr[k], j);
+        int okj = 1;
+        if (lane == j) {
+            double s = A[j * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) s = s - Lr[k] * Lr[k];
+            okj = (s > 0.0) && finite_d(s);
+            Lr[j] = sqrt(s);
+        }
+        const double d = __shfl_sync(kFull, Lr[j], j);
+        okj = __shfl_sync(kFull, okj, j);
+        if (lane > j && lane < 6) {
+            double t = A[lane * 6 + j];
+#pragma unroll
+            for (int k = 0; k < j; ++k) t = t - Lr[k] * Lj[k];
+            Lr[j] = t / d;
+        }
+        if (!okj) {
+            factored = false;
+            return false;
+        }
+    }
+    factored = true;
+    if (lane < 6) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) Ls[lane * 6 + c] = Lr[c];
+    }
+    __syncwarp();
+    if (lane < 6) {
+        const int c = lane;
+        double Lc[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+            Lc[i] = 0.0;
+            if (i == c) {
+                Lc[i] = 1.0 / Ls[i * 6 + i];
+            } else if (i > c) {
+                double t = 0.0;
+#pragma unroll
+                for (int k = 0; k < i; ++k)
+                    if (k >= c) t = t + Ls[i * 6 + k] * Lc[k];
+                Lc[i] = -t / Ls[i * 6 + i];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) Lis[i * 6 + c] = Lc[i];
+    }
+    __syncwarp();
+    bool ok = true;
+    if (lane < 21) {
+        int r = 0, m = lane;
+        while (m >= 6 - r) {
+            m -= 6 - r;
+            ++r;
+        }
+        const int c = r + m;
+        double t = 0.0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            if (k >= c) t = t + Lis[k * 6 + r] * Lis[k * 6 + c];
+        Ai[r * 6 + c] = t;
+        Ai[c * 6 + r] = t;
+        ok = finite_d(t);
+    }
+    ok = __all_sync(kFull, ok);
+    __syncwarp();
+    return ok;
+}
+
+// well_conditioned_r on H (shared memory); scr: 180 doubles.
+__device__ __forceinline__ bool well_conditioned_warp(const double* H, int half, double* scr) {
+    const int lane = threadIdx.x & 31;
+    double* Hn = scr;
+    double* Hi = scr + 36;
+    double* sub = scr + 72;
+    const double s = half > 1 ? 1.0 / (double)half : 1.0;
+    bool fin = true;
+    for (int e = lane; e < 36; e += 32) {
+        const int r = e / 6, c = e - (e / 6) * 6;
+        const double dr = r < 2 ? 1.0 : s, dc = c < 2 ? 1.0 : s;
+        const double h = (dr * H[e]) * dc;
+        Hn[e] = h;
+        fin = fin && finite_d(h);
+    }
+    fin = __all_sync(kFull, fin);
+    __syncwarp();
+    if (!fin) return false;
+    bool factored;
+    if (!inverse6_warp(Hn, Hi, sub, factored)) return false;
+    double a = 0.0, b = 0.0;
+    if (lane < 6) {
+#pragma unroll
+        for (int r = 0; r < 6; ++r) {
+            a = a + fabs(Hn[r * 6 + lane]);
+            b = b + fabs(Hi[r * 6 + lane]);
+        }
+    }
+    // the largest column sums; fmax of non-negative, non-NaN values in any order
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) {
+        a = fmax(a, __shfl_xor_sync(kFull, a, o));
+        b = fmax(b, __shfl_xor_sync(kFull, b, o));
+    }
+    const double na = __shfl_sync(kFull, a, 0), ni = __shfl_sync(kFull, b, 0);
+    __syncwarp();
+    return 1.0 / (na * ni) > (double)1e-6f;
+}
+
 __device__ __forceinline__ bool cond2x2_ok(const double (&H)[6][6]) {
     const double det = H[0][0] * H[1][1] - H[1][0] * H[0][1];
     const double nrm = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[1][0] * H[1][0] + H[1][1] * H[1][1];
@@ -278,5 +408,15 @@ __device__ __forceinline__ bool cond2x2_ok(const double (&H)[6][6]) {
 
 // Index of (r, c), r <= c, in the 21-entry upper triangle (row-major).
 __host__ __device__ constexpr int tri21(int r, int c) { return r * 6 - (r * (r - 1)) / 2 + (c - r); }
+// The row and column of upper-triangle entry m (the inverse of tri21).
+__host__ __device__ constexpr int tri_row(int m) {
+    int r = 0;
+    while (m >= 6 - r) {
+        m -= 6 - r;
+        ++r;
+    }
+    return r;
+}
+__host__ __device__ constexpr int tri_col(int m) { return tri_row(m) + (m - tri21(tri_row(m), tri_row(m))); }
 
 }  // namespace dic

@@ -800,15 +800,31 @@ struct StagedLayout {
 };
 
 // The cooperative rescue: warp 0 of a block drives a task, and every warp of
-// the block samples a share of the subset for each evaluation.
+// the block samples a share of the subset for each evaluation; the masked
+// iteration's Hessian and its inversion run on the other warps.
 constexpr int kCoopWarps = 8;
 struct CoopReq {
-    int op;  // 0: done, 1: sample, 2: coarse search, 3: stage the reference subset
+    // 0: done, 1: sample, 2: coarse search, 3: stage the reference subset,
+    // 4: masked-iteration step matrix, 5: ZNSSD residuals
+    int op;
     int cx, cy, tile_ok, tx0, ty0;
     float Wp[6];
     float mref, iref;
+    float mean, inv, sdev;  // op 5: the warped subset's statistics
+    int full;
 };
-constexpr int kCoopBytes = 64 + kCoopWarps * 32 * 8 + kCoopWarps * 8;
+// The request block's layout: request, guard bits (kCoopWarps x 32 masks),
+// coarse-search slots, the masked Hessian's 21 sums, its flags, and the
+// scratch of the two warps that invert it.
+constexpr int kCoopGbits = 128;
+static_assert(sizeof(CoopReq) <= kCoopGbits, "request block");
+constexpr int kCoopSlots = kCoopGbits + kCoopWarps * 32 * 8;
+constexpr int kCoopHsum = kCoopSlots + kCoopWarps * 8;
+constexpr int kCoopFlags = kCoopHsum + 176;
+constexpr int kCoopScrCond = kCoopFlags + 16;        // 36 + 180 doubles
+constexpr int kCoopScrInv = kCoopScrCond + 216 * 8;  // 36 + 72 doubles
+constexpr int kCoopBytes = kCoopScrInv + 108 * 8;
+static_assert(kCoopHsum % 8 == 0 && kCoopScrCond % 8 == 0, "double alignment");
 
 // stage false: no staged reference subset (the solver reads the planes);
 // coop: room for the cooperative rescue's request block
@@ -879,6 +895,10 @@ struct WarpSolver {
     CoopReq* req;
     Mask* gbits;
     float2* cslots;
+    double* hsum;  // the masked Hessian's upper triangle (21)
+    int* mflags;   // [0] 2x2 test, [1] conditioning, [2] inversion
+    double* scr_cond;
+    double* scr_inv;
     int warp;
 
     __device__ __forceinline__ void advance(int& row, int& col) const {
@@ -1102,7 +1122,12 @@ struct WarpSolver {
             lo_y = (float)(4 - cy);
             hi_y = (float)(H - 4 - cy);
             ref_base = (cy - half + ref_dy) * ref_pitch + (cx - half + ref_dx);
-            if (op == 3) {
+            if (op == 5) {
+                const int lo = warp * per, hi = min(K, lo + per);
+                residual_part(lo, hi, gbits[lane], req->mean, req->inv, req->sdev, req->full != 0);
+            } else if (op == 4) {
+                masked_serve();
+            } else if (op == 3) {
                 mref = req->mref;
                 iref = req->iref;
                 const int lo = warp * per, hi = min(K, lo + per);
@@ -1157,15 +1182,18 @@ struct WarpSolver {
 #pragma unroll
             for (int w = 1; w < kCoopWarps; ++w) g |= gbits[w * 32 + lane];
             valid = g & refok;
+            // the ordered sum with every load issued ahead of its add (the
+            // add is kept for valid pixels only: same bits as skipping)
             float part = 0.0f;
-            int cnt = 0;
-            for (int k = 0; k < K; ++k)
-                if ((valid >> k) & 1u) {
-                    part = part + vals[lane + 32 * k];
-                    ++cnt;
-                }
+#pragma unroll 8
+            for (int k = 0; k < K; ++k) {
+                const int i = lane + 32 * k;
+                const float v = vals[i < n ? i : 0];
+                const float p2 = part + v;
+                part = ((valid >> k) & 1u) ? p2 : part;
+            }
             sum = wsum(part);
-            return wsum(cnt);
+            return wsum(__popcll((unsigned long long)valid));
         }
         if constexpr (!STAGE && !COOP) {
             // the fast pass's common case: every sample inside the guard and
@@ -1255,11 +1283,22 @@ struct WarpSolver {
 
     __device__ __forceinline__ float sum_sq(float mean, Mask valid) const {
         float sq = 0.0f;
+        if constexpr (COOP) {
+            // every load issued ahead of its fused add, kept for valid pixels
+#pragma unroll 8
+            for (int k = 0; k < K; ++k) {
+                const int i = lane + 32 * k;
+                const float d = vals[i < n ? i : 0] - mean;
+                const float s2 = __fmaf_rn(d, d, sq);
+                sq = ((valid >> k) & 1u) ? s2 : sq;
+            }
+        } else {
 #pragma unroll 4
-        for (int k = 0; k < K; ++k) {
-            if (!((valid >> k) & 1u)) continue;
-            const float d = vals[lane + 32 * k] - mean;
-            sq = __fmaf_rn(d, d, sq);
+            for (int k = 0; k < K; ++k) {
+                if (!((valid >> k) & 1u)) continue;
+                const float d = vals[lane + 32 * k] - mean;
+                sq = __fmaf_rn(d, d, sq);
+            }
         }
         return wsum(sq);
     }
@@ -1313,6 +1352,79 @@ struct WarpSolver {
         return ok != 0;
     }
 
+    // COOP, warps 1..7: three of the masked Hessian's 21 sums (upper-triangle
+    // entries M0..M0+2), each with the operations and order of masked_step.
+    template <int M0>
+    __device__ __forceinline__ void masked_sums3(Mask valid) {
+        constexpr int a0 = tri_row(M0), b0 = tri_col(M0), a1 = tri_row(M0 + 1), b1 = tri_col(M0 + 1);
+        constexpr int a2 = tri_row(M0 + 2), b2 = tri_col(M0 + 2);
+        double h0 = 0.0, h1 = 0.0, h2 = 0.0;
+        int row = row0, col = col0;
+        for (int k = 0; k < K; ++k) {
+            if ((valid >> k) & 1u) {
+                const int i = lane + 32 * k;
+                const float g0 = gx_at(i, row, col) * iref, g1 = gy_at(i, row, col) * iref;
+                const float fx = (float)(col - half), fy = (float)(row - half);
+                const double s[6] = {(double)g0, (double)g1, (double)(g0 * fx), (double)(g0 * fy),
+                                     (double)(g1 * fx), (double)(g1 * fy)};
+                h0 = __fma_rn(s[a0], s[b0], h0);
+                h1 = __fma_rn(s[a1], s[b1], h1);
+                h2 = __fma_rn(s[a2], s[b2], h2);
+            }
+            advance(row, col);
+        }
+        h0 = wsum(h0);
+        h1 = wsum(h1);
+        h2 = wsum(h2);
+        if (lane == 0) {
+            hsum[M0] = h0;
+            hsum[M0 + 1] = h1;
+            hsum[M0 + 2] = h2;
+        }
+    }
+
+    // COOP, warps 1..7: the masked iteration's step matrix (masked_step's
+    // Hessian, tests and inverse) into Hm, its verdicts into mflags. Warp 1
+    // runs the 2x2 test and the conditioning, warp 2 the inversion, at the
+    // same time.
+    __device__ void masked_serve() {
+        const Mask valid = gbits[lane];
+        switch (warp) {
+            case 1: masked_sums3<0>(valid); break;
+            case 2: masked_sums3<3>(valid); break;
+            case 3: masked_sums3<6>(valid); break;
+            case 4: masked_sums3<9>(valid); break;
+            case 5: masked_sums3<12>(valid); break;
+            case 6: masked_sums3<15>(valid); break;
+            default: masked_sums3<18>(valid); break;
+        }
+        asm volatile("bar.sync 2, %0;" ::"n"((kCoopWarps - 1) * 32) : "memory");
+        if (warp != 1 && warp != 2) return;
+        double* Hd = warp == 1 ? scr_cond : scr_inv;
+        for (int e = lane; e < 36; e += 32) {
+            const int rr = e / 6, cc = e - (e / 6) * 6;
+            double h = hsum[rr <= cc ? tri21(rr, cc) : tri21(cc, rr)];
+            if (lm && rr == cc && rr < 2) h += (double)kLmAlpha;
+            Hd[e] = h;
+        }
+        __syncwarp();
+        if (warp == 1) {
+            if (lane == 0) {
+                double H2[6][6];
+                H2[0][0] = hsum[tri21(0, 0)];
+                H2[0][1] = H2[1][0] = hsum[tri21(0, 1)];
+                H2[1][1] = hsum[tri21(1, 1)];
+                mflags[0] = cond2x2_ok(H2) ? 1 : 0;
+            }
+            const bool wc = well_conditioned_warp(Hd, half, scr_cond + 36);
+            if (lane == 0) mflags[1] = wc ? 1 : 0;
+        } else {
+            bool factored;
+            const bool ok = inverse6_warp(Hd, Hm, scr_inv + 36, factored);
+            if (lane == 0) mflags[2] = ok ? 1 : 0;
+        }
+    }
+
     // solve_icgn (optimization_engine.cpp:272-465). With GENERAL false a
     // masked iteration is not taken: `defer` is set instead.
     template <bool GENERAL>
@@ -1329,6 +1441,14 @@ struct WarpSolver {
                 if (!full) {
                     defer = true;
                     return res_from(Wp, 1, 2.0f, iter);
+                }
+            }
+            if constexpr (GENERAL && COOP) {
+                // the other warps form the masked iteration's step matrix
+                // while this one forms the residual sums
+                if (!full) {
+                    gbits[lane] = valid;
+                    coop_post(4, nullptr);
                 }
             }
             const float mean = sum / (float)cnt;
@@ -1423,7 +1543,12 @@ struct WarpSolver {
             const double* Hstep = Hr;
             if constexpr (GENERAL) {
                 if (!full) {
-                    if (!masked_step(valid)) return res_from(Wp, 1, 2.0f, iter);
+                    if constexpr (COOP) {
+                        coop_bar();  // the step matrix is formed
+                        if (!(mflags[0] && mflags[1] && mflags[2])) return res_from(Wp, 1, 2.0f, iter);
+                    } else {
+                        if (!masked_step(valid)) return res_from(Wp, 1, 2.0f, iter);
+                    }
                     Hstep = Hm;
                 }
             }
@@ -1495,6 +1620,19 @@ struct WarpSolver {
         return res_from(Wp, 1, final_score, kIcgnMaxIter);
     }
 
+    // COOP: the ZNSSD residuals of pixels k in [k_lo, k_hi) of this lane, in
+    // place of their values (evaluate_znssd's per-pixel difference).
+    __device__ __forceinline__ void residual_part(int k_lo, int k_hi, Mask valid, float mean, float inv, float sdev,
+                                                  bool full) {
+        for (int k = k_lo; k < k_hi; ++k) {
+            if ((valid >> k) & 1u) {
+                const int i = lane + 32 * k;
+                const float rn = srn[i];
+                vals[i] = full ? rn - (vals[i] - mean) * inv : rn - (vals[i] - mean) / sdev;
+            }
+        }
+    }
+
     // evaluate_znssd (optimization_engine.cpp:467-528).
     __device__ __forceinline__ float znssd(const float Wp[6]) {
         float sum;
@@ -1507,6 +1645,30 @@ struct WarpSolver {
         const bool full = cnt == n;
         const float inv = 1.0f / sdev;
         float ep = 0.0f;
+        if constexpr (COOP) {
+            // every warp forms the residuals of its share (each with its own
+            // division), then this warp sums their squares in pixel order
+            const int per = (K + kCoopWarps - 1) / kCoopWarps;
+            gbits[lane] = valid;
+            if (lane == 0) {
+                req->mean = mean;
+                req->inv = inv;
+                req->sdev = sdev;
+                req->full = full ? 1 : 0;
+            }
+            coop_post(5, nullptr);
+            residual_part(0, min(K, per), valid, mean, inv, sdev, full);
+            coop_bar();
+#pragma unroll 8
+            for (int k = 0; k < K; ++k) {
+                const int i = lane + 32 * k;
+                const float d = vals[i < n ? i : 0];
+                const float e = __fmaf_rn(d, d, ep);
+                ep = ((valid >> k) & 1u) ? e : ep;
+            }
+            const float score = wsum(ep) / (float)cnt;
+            return finite_f(score) ? score : 2.0f;
+        }
         int row = row0, col = col0;
 #pragma unroll 4
         for (int k = 0; k < K; ++k) {
@@ -1787,8 +1949,12 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
     s.phase = 0;
     s.warp = (int)(threadIdx.x >> 5);
     s.req = reinterpret_cast<CoopReq*>(smem + L.off_coop);
-    s.gbits = reinterpret_cast<Mask*>(smem + L.off_coop + 64);
-    s.cslots = reinterpret_cast<float2*>(smem + L.off_coop + 64 + kCoopWarps * 32 * 8);
+    s.gbits = reinterpret_cast<Mask*>(smem + L.off_coop + kCoopGbits);
+    s.cslots = reinterpret_cast<float2*>(smem + L.off_coop + kCoopSlots);
+    s.hsum = reinterpret_cast<double*>(smem + L.off_coop + kCoopHsum);
+    s.mflags = reinterpret_cast<int*>(smem + L.off_coop + kCoopFlags);
+    s.scr_cond = reinterpret_cast<double*>(smem + L.off_coop + kCoopScrCond);
+    s.scr_inv = reinterpret_cast<double*>(smem + L.off_coop + kCoopScrInv);
     // one barrier per block, set up by its first warp (the driver, with COOP)
     if (threadIdx.x == 0) mbar_init(s.bar, 1);
     fence_proxy_async_smem();

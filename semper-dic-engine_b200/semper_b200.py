@@ -38,7 +38,7 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
                "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion",
                "semper_b200_batch_create", "semper_b200_batch_destroy", "semper_b200_batch_run",
-               "semper_b200_batch_last_error", "semper_b200_incremental_profile"]
+               "semper_b200_batch_last_error", "semper_b200_incremental_profile", "semper_b200_fast_pass_shape"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -104,6 +104,7 @@ def lib():
         L.semper_b200_stream.restype = _vp
         L.semper_b200_last_timings.argtypes = [_vp, _f32p, ctypes.POINTER(ctypes.c_longlong)]
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
+        L.semper_b200_fast_pass_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
         L.semper_b200_set_global_motion.argtypes = [_vp, ctypes.c_int]
         L.semper_b200_batch_create.argtypes = [ctypes.c_int32]
         L.semper_b200_batch_create.restype = _vp
@@ -212,6 +213,11 @@ class Engine:
         names = ["prep", "pool", "seed", "mesh", "path_a", "path_b", "strain", "total"]
         counts = ["icgn_iters", "pixel_iters", "path_a_tasks", "path_a_pixel_iters", "launches"]
         return dict(zip(names, map(float, t))), dict(zip(counts, map(int, c)))
+
+    def fast_pass_shape(self, subset_size: int, six: bool = False) -> int:
+        """The Path A fast pass's shape the autotuner kept: 0 reference read
+        from the planes, 1 staged in shared memory, -1 not decided yet."""
+        return lib().semper_b200_fast_pass_shape(self._h, subset_size, 1 if six else 0)
 
     def set_global_model(self, H=None) -> int:
         Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
