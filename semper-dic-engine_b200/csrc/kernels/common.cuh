@@ -144,6 +144,42 @@ __device__ __forceinline__ float interp6s(const float* base, int pitch, int xi, 
     return val;
 }
 
+// Two pixels at once on the paired FP32 instructions of sm_100 (each half an
+// IEEE single-precision operation rounded to nearest, so every value is the
+// one the scalar form gives): the Catmull-Rom weights of two offsets and
+// interp4s of two samples from the same tile.
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+__device__ __forceinline__ void cubic_weights_x2(float2 s, float2 w[4]) {
+    const float2 s2 = __fmul2_rn(s, s), s3 = __fmul2_rn(s2, s);
+    w[0] = __ffma2_rn(f2(-0.5f), s, __ffma2_rn(f2(-0.5f), s3, s2));
+    w[1] = __ffma2_rn(f2(-2.5f), s2, __ffma2_rn(f2(1.5f), s3, f2(1.0f)));
+    w[2] = __ffma2_rn(f2(0.5f), s, __ffma2_rn(f2(-1.5f), s3, __fmul2_rn(f2(2.0f), s2)));
+    w[3] = __ffma2_rn(f2(0.5f), s3, __fmul2_rn(f2(-0.5f), s2));
+}
+
+// Pixel A at (xa + dx.x, ya + dy.x), pixel B at (xb + dx.y, yb + dy.y).
+__device__ __forceinline__ float2 interp4s_x2(const float* base, int pitch, int xa, int ya, int xb, int yb, float2 dx,
+                                              float2 dy) {
+    float2 wx[4], wy[4];
+    cubic_weights_x2(dx, wx);
+    cubic_weights_x2(dy, wy);
+    const float* ra = base + (ya - 1) * pitch + (xa - 1);
+    const float* rb = base + (yb - 1) * pitch + (xb - 1);
+    float2 val = f2(0.0f);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const float* qa = ra + j * pitch;
+        const float* qb = rb + j * pitch;
+        float2 rv = __fmul2_rn(make_float2(qa[0], qb[0]), wx[0]);
+        rv = __ffma2_rn(make_float2(qa[1], qb[1]), wx[1], rv);
+        rv = __ffma2_rn(make_float2(qa[2], qb[2]), wx[2], rv);
+        rv = __ffma2_rn(make_float2(qa[3], qb[3]), wx[3], rv);
+        val = (j == 0) ? __fmul2_rn(rv, wy[0]) : __ffma2_rn(rv, wy[j], val);
+    }
+    return val;
+}
+
 // The 6x6 FP64 helpers of the Hessian: Cholesky, explicit inverse, and the
 // scaled 1-norm reciprocal condition (src/math/hessian.hpp:40-52). The `_r`
 // forms are fully unrolled, so their matrices live in registers; the

@@ -1202,29 +1202,71 @@ struct WarpSolver {
             if (all_in && tile_ok && ghost == 0) {
                 float part = 0.0f;
                 int row = row0, col = col0;
-                for (int k0 = 0; k0 < K; k0 += 4) {
-                    float v[4];
-                    int ii[4];
+                if constexpr (!SIX) {
+                    // two pixels per paired FP32 instruction; a pixel past
+                    // the subset samples the centre (inside the tile) and is
+                    // dropped
+                    const float2 W0 = f2(Wp[0]), W1 = f2(Wp[1]), W2 = f2(Wp[2]);
+                    const float2 W3 = f2(Wp[3]), W4 = f2(Wp[4]), W5 = f2(Wp[5]);
+                    const int bx = cx - tx0, by = cy - ty0;
+                    for (int k0 = 0; k0 < K; k0 += 4) {
+                        float v[4], ox[4], oy[4];
+                        int ii[4];
+                        bool ok[4];
 #pragma unroll
-                    for (int u = 0; u < 4; ++u) {
-                        const int k = k0 + u;
-                        ii[u] = lane + 32 * k;
-                        v[u] = 0.0f;
-                        if (k < K && ii[u] < n) {
-                            const float ox = (float)(col - half), oy = (float)(row - half);
-                            const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
-                            const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
-                            const float flx = floorf(fx), fly = floorf(fy);
-                            const int lx = cx + (int)flx - tx0, ly = cy + (int)fly - ty0;
-                            v[u] = SIX ? interp6s(tile, tw, lx, ly, fx - flx, fy - fly)
-                                       : interp4s(tile, tw, lx, ly, fx - flx, fy - fly);
-                            part = part + v[u];
+                        for (int u = 0; u < 4; ++u) {
+                            const int k = k0 + u;
+                            ii[u] = lane + 32 * k;
+                            ok[u] = k < K && ii[u] < n;
+                            ox[u] = ok[u] ? (float)(col - half) : 0.0f;
+                            oy[u] = ok[u] ? (float)(row - half) : 0.0f;
+                            advance(row, col);
                         }
-                        advance(row, col);
-                    }
 #pragma unroll
-                    for (int u = 0; u < 4; ++u)
-                        if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
+                        for (int u = 0; u < 4; u += 2) {
+                            const float2 OX = make_float2(ox[u], ox[u + 1]), OY = make_float2(oy[u], oy[u + 1]);
+                            const float2 FX = __ffma2_rn(W0, OX, __ffma2_rn(W1, OY, W2));
+                            const float2 FY = __ffma2_rn(W3, OX, __ffma2_rn(W4, OY, W5));
+                            const float2 FLX = make_float2(floorf(FX.x), floorf(FX.y));
+                            const float2 FLY = make_float2(floorf(FY.x), floorf(FY.y));
+                            // fx - floor(fx) as one rounding: fma(floor, -1, fx)
+                            const float2 V = interp4s_x2(tile, tw, bx + (int)FLX.x, by + (int)FLY.x, bx + (int)FLX.y,
+                                                         by + (int)FLY.y, __ffma2_rn(FLX, f2(-1.0f), FX),
+                                                         __ffma2_rn(FLY, f2(-1.0f), FY));
+                            v[u] = V.x;
+                            v[u + 1] = V.y;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (ok[u]) {
+                                part = part + v[u];
+                                vals[ii[u]] = v[u];
+                            }
+                    }
+                } else {
+                    for (int k0 = 0; k0 < K; k0 += 4) {
+                        float v[4];
+                        int ii[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            const int k = k0 + u;
+                            ii[u] = lane + 32 * k;
+                            v[u] = 0.0f;
+                            if (k < K && ii[u] < n) {
+                                const float ox = (float)(col - half), oy = (float)(row - half);
+                                const float fx = __fmaf_rn(Wp[0], ox, __fmaf_rn(Wp[1], oy, Wp[2]));
+                                const float fy = __fmaf_rn(Wp[3], ox, __fmaf_rn(Wp[4], oy, Wp[5]));
+                                const float flx = floorf(fx), fly = floorf(fy);
+                                const int lx = cx + (int)flx - tx0, ly = cy + (int)fly - ty0;
+                                v[u] = interp6s(tile, tw, lx, ly, fx - flx, fy - fly);
+                                part = part + v[u];
+                            }
+                            advance(row, col);
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u)
+                            if (k0 + u < K && ii[u] < n) vals[ii[u]] = v[u];
+                    }
                 }
                 __syncwarp();
                 valid = fullmask;
@@ -1461,21 +1503,6 @@ struct WarpSolver {
             // pixels in the same order, taken here where the gradients are
             // loaded anyway (reference read from the planes)
             float tsx = 0.0f, tsy = 0.0f;
-            // one pixel's share of the residual and the steepest-descent sums
-            auto accumulate = [&](int i, float I, float gx, float gy, float fx, float fy) {
-                tsx = __fmaf_rn(gx, gx, tsx);
-                tsy = __fmaf_rn(gy, gy, tsy);
-                const float rn = (I - mref) * iref, g0 = gx * iref, g1 = gy * iref;
-                const float nd = (vals[i] - mean) * inv;
-                const float diff = rn - nd;
-                ep = __fmaf_rn(diff, diff, ep);
-                gp0 = __fmaf_rn(g0, diff, gp0);
-                gp1 = __fmaf_rn(g1, diff, gp1);
-                gp2 = __fmaf_rn(g0 * fx, diff, gp2);
-                gp3 = __fmaf_rn(g0 * fy, diff, gp3);
-                gp4 = __fmaf_rn(g1 * fx, diff, gp4);
-                gp5 = __fmaf_rn(g1 * fy, diff, gp5);
-            };
             if constexpr (STAGE) {
                 int row = row0, col = col0;
 #pragma unroll 4
@@ -1518,6 +1545,28 @@ struct WarpSolver {
                         advance(lr, lc);
                     }
                 };
+                // One pixel's share of the residual and steepest-descent sums,
+                // independent sums in pairs on the paired FP32 instructions:
+                // (tsx, tsy), (gp0, gp1), (gp2, gp4), (gp3, gp5). Per sum:
+                // ts += g g; rn = (I - mref) iref; nd = (v - mean) inv;
+                // diff = rn - nd; ep += diff^2; gp0 += g0 diff, gp1 += g1 diff,
+                // gp2 += (g0 fx) diff, gp3 += (g0 fy) diff, gp4 += (g1 fx)
+                // diff, gp5 += (g1 fy) diff, with g0 = gx iref, g1 = gy iref.
+                float2 TS = f2(0.0f), GP01 = f2(0.0f), GP24 = f2(0.0f), GP35 = f2(0.0f);
+                const float2 NEG = make_float2(-mref, -mean), SCL = make_float2(iref, inv);
+                auto accumulate2 = [&](int i, float I, float gx, float gy, float fx, float fy) {
+                    const float2 GXY = make_float2(gx, gy);
+                    TS = __ffma2_rn(GXY, GXY, TS);
+                    // (rn, nd) = ((I - mref) * iref, (vals[i] - mean) * inv)
+                    const float2 RN = __fmul2_rn(__fadd2_rn(make_float2(I, vals[i]), NEG), SCL);
+                    const float diff = RN.x - RN.y;
+                    const float2 G01 = __fmul2_rn(GXY, f2(iref));  // (g0, g1)
+                    const float2 D = f2(diff);
+                    ep = __fmaf_rn(diff, diff, ep);
+                    GP01 = __ffma2_rn(G01, D, GP01);
+                    GP24 = __ffma2_rn(__fmul2_rn(G01, f2(fx)), D, GP24);  // (g0 fx, g1 fx)
+                    GP35 = __ffma2_rn(__fmul2_rn(G01, f2(fy)), D, GP35);  // (g0 fy, g1 fy)
+                };
                 fetch(0);
                 for (int k0 = 0; k0 < K; k0 += G) {
                     float cI[G], cX[G], cY[G], cfx[G], cfy[G];
@@ -1533,9 +1582,17 @@ struct WarpSolver {
 #pragma unroll
                     for (int u = 0; u < G; ++u) {
                         const int k = k0 + u;
-                        if (k < K && ((valid >> k) & 1u)) accumulate(lane + 32 * k, cI[u], cX[u], cY[u], cfx[u], cfy[u]);
+                        if (k < K && ((valid >> k) & 1u)) accumulate2(lane + 32 * k, cI[u], cX[u], cY[u], cfx[u], cfy[u]);
                     }
                 }
+                tsx = TS.x;
+                tsy = TS.y;
+                gp0 = GP01.x;
+                gp1 = GP01.y;
+                gp2 = GP24.x;
+                gp4 = GP24.y;
+                gp3 = GP35.x;
+                gp5 = GP35.y;
             }
             const float err2 = wsum(ep);
             const float g[6] = {wsum(gp0), wsum(gp1), wsum(gp2), wsum(gp3), wsum(gp4), wsum(gp5)};
