@@ -1202,7 +1202,42 @@ struct WarpSolver {
             if (all_in && tile_ok && ghost == 0) {
                 float part = 0.0f;
                 int row = row0, col = col0;
-                if constexpr (!SIX) {
+                if (!SIX && dim == 31) {
+                    // Subset 31: lane c samples column c of every row (lane 31
+                    // idle), two rows per paired FP32 instruction, so the taps
+                    // of a warp lie on one tile row and hit 31 distinct banks
+                    // (the sums' layout puts a 32nd pixel on the next row,
+                    // which the tile's 16-byte row pitch makes collide). The
+                    // values go to vals; the ordered sum then reads them in
+                    // the sums' layout.
+                    const float2 W0 = f2(Wp[0]), W1 = f2(Wp[1]), W2 = f2(Wp[2]);
+                    const float2 W3 = f2(Wp[3]), W4 = f2(Wp[4]), W5 = f2(Wp[5]);
+                    const int bx = cx - tx0, by = cy - ty0;
+                    const bool act = lane < 31;
+                    const float2 OX = f2((float)((act ? lane : half) - half));
+#pragma unroll 2
+                    for (int r0 = 0; r0 < 31; r0 += 2) {
+                        const int r1 = r0 + 1 < 31 ? r0 + 1 : r0;
+                        const float2 OY = make_float2((float)(r0 - half), (float)(r1 - half));
+                        const float2 FX = __ffma2_rn(W0, OX, __ffma2_rn(W1, OY, W2));
+                        const float2 FY = __ffma2_rn(W3, OX, __ffma2_rn(W4, OY, W5));
+                        const float2 FLX = make_float2(floorf(FX.x), floorf(FX.y));
+                        const float2 FLY = make_float2(floorf(FY.x), floorf(FY.y));
+                        const float2 V = interp4s_x2(tile, tw, bx + (int)FLX.x, by + (int)FLY.x, bx + (int)FLX.y,
+                                                     by + (int)FLY.y, __ffma2_rn(FLX, f2(-1.0f), FX),
+                                                     __ffma2_rn(FLY, f2(-1.0f), FY));
+                        if (act) {
+                            vals[r0 * 31 + lane] = V.x;
+                            if (r1 != r0) vals[r1 * 31 + lane] = V.y;
+                        }
+                    }
+                    __syncwarp();
+#pragma unroll 8
+                    for (int k = 0; k < K; ++k) {
+                        const int i = lane + 32 * k;
+                        if (i < n) part = part + vals[i];
+                    }
+                } else if constexpr (!SIX) {
                     // two pixels per paired FP32 instruction; a pixel past
                     // the subset samples the centre (inside the tile) and is
                     // dropped
