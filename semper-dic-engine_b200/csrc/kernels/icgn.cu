@@ -28,6 +28,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -794,6 +795,7 @@ constexpr int kFastMaxPerLane = 64;  // n <= 2048 (subset <= 45); larger subsets
 constexpr int kFastMaxSmem = 227 * 1024;
 
 struct StagedLayout {
+    int tile_w, tile_h;  // the tile box the layout holds
     int off_tile, off_vals, off_rn, off_gx, off_gy;
     int off_coop;  // the cooperative rescue's request block and guard bits (0: none)
     int bytes;     // per warp (per block for the cooperative rescue), a multiple of 128
@@ -830,6 +832,8 @@ static_assert(kCoopHsum % 8 == 0 && kCoopScrCond % 8 == 0, "double alignment");
 // coop: room for the cooperative rescue's request block
 StagedLayout staged_layout(int n, int tw, int th, bool stage = true, bool coop = false) {
     StagedLayout L;
+    L.tile_w = tw;
+    L.tile_h = th;
     L.off_tile = 640;
     int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
     const int arr = (n * 4 + 15) & ~15;
@@ -1182,16 +1186,10 @@ struct WarpSolver {
 #pragma unroll
             for (int w = 1; w < kCoopWarps; ++w) g |= gbits[w * 32 + lane];
             valid = g & refok;
-            // the ordered sum with every load issued ahead of its add (the
-            // add is kept for valid pixels only: same bits as skipping)
             float part = 0.0f;
-#pragma unroll 8
-            for (int k = 0; k < K; ++k) {
-                const int i = lane + 32 * k;
-                const float v = vals[i < n ? i : 0];
-                const float p2 = part + v;
-                part = ((valid >> k) & 1u) ? p2 : part;
-            }
+#pragma unroll 4
+            for (int k = 0; k < K; ++k)
+                if ((valid >> k) & 1u) part = part + vals[lane + 32 * k];
             sum = wsum(part);
             return wsum(__popcll((unsigned long long)valid));
         }
@@ -1360,22 +1358,11 @@ struct WarpSolver {
 
     __device__ __forceinline__ float sum_sq(float mean, Mask valid) const {
         float sq = 0.0f;
-        if constexpr (COOP) {
-            // every load issued ahead of its fused add, kept for valid pixels
-#pragma unroll 8
-            for (int k = 0; k < K; ++k) {
-                const int i = lane + 32 * k;
-                const float d = vals[i < n ? i : 0] - mean;
-                const float s2 = __fmaf_rn(d, d, sq);
-                sq = ((valid >> k) & 1u) ? s2 : sq;
-            }
-        } else {
 #pragma unroll 4
-            for (int k = 0; k < K; ++k) {
-                if (!((valid >> k) & 1u)) continue;
-                const float d = vals[lane + 32 * k] - mean;
-                sq = __fmaf_rn(d, d, sq);
-            }
+        for (int k = 0; k < K; ++k) {
+            if (!((valid >> k) & 1u)) continue;
+            const float d = vals[lane + 32 * k] - mean;
+            sq = __fmaf_rn(d, d, sq);
         }
         return wsum(sq);
     }
@@ -1437,6 +1424,7 @@ struct WarpSolver {
         constexpr int a2 = tri_row(M0 + 2), b2 = tri_col(M0 + 2);
         double h0 = 0.0, h1 = 0.0, h2 = 0.0;
         int row = row0, col = col0;
+#pragma unroll 4
         for (int k = 0; k < K; ++k) {
             if ((valid >> k) & 1u) {
                 const int i = lane + 32 * k;
@@ -1751,12 +1739,11 @@ struct WarpSolver {
             coop_post(5, nullptr);
             residual_part(0, min(K, per), valid, mean, inv, sdev, full);
             coop_bar();
-#pragma unroll 8
+#pragma unroll 4
             for (int k = 0; k < K; ++k) {
-                const int i = lane + 32 * k;
-                const float d = vals[i < n ? i : 0];
-                const float e = __fmaf_rn(d, d, ep);
-                ep = ((valid >> k) & 1u) ? e : ep;
+                if (!((valid >> k) & 1u)) continue;
+                const float d = vals[lane + 32 * k];
+                ep = __fmaf_rn(d, d, ep);
             }
             const float score = wsum(ep) / (float)cnt;
             return finite_f(score) ? score : 2.0f;
@@ -2161,8 +2148,8 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
                                                                          const SolveArgs a, const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
     WarpSolver<SIX, uint64_t, true, true> s;
-    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, a.tile_w,
-                 a.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, L.tile_w,
+                 L.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
     if (s.warp != 0) {
         s.coop_serve();
         return;
@@ -2314,8 +2301,8 @@ cudaError_t one_wave(K kernel, size_t smem, long cap, long tasks, long& blocks, 
 // The fast pass and then the rescue pass over what it handed on; subsets the
 // staged solvers do not take go to solve_kernel, which takes every task.
 template <bool SIX>
-cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const StagedLayout& SL, bool staged_ok,
-                          int grid_blocks, size_t smem, cudaStream_t st) {
+cudaError_t launch_passes(const CUtensorMap& tmap, const CUtensorMap& tmap_r, int tw_r, int th_r, const SolveArgs& a,
+                          const StagedLayout& SL, bool staged_ok, int grid_blocks, size_t smem, cudaStream_t st) {
     // the caller's hint counts units of kSolveThreads / 32 subsets
     const long cap = grid_blocks > 0 ? (long)grid_blocks * (kSolveThreads / 32) : 0;
     long blocks = 1;
@@ -2341,13 +2328,14 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const SolveArgs& a, const Sta
             if (e != cudaSuccess) return e;
             fast<<<(unsigned)blocks, 32, FL.bytes, st>>>(tmap, a, FL);
         }
-        // the rescue pass: a block of kCoopWarps warps per task
-        const StagedLayout RL = staged_layout(a.n, a.tile_w, a.tile_h, true, true);
+        // the rescue pass: a block of kCoopWarps warps per task, with its own
+        // larger tile (one block per SM leaves the shared memory for it)
+        const StagedLayout RL = staged_layout(a.n, tw_r, th_r, true, true);
         e = allow_max_smem(coop_rescue_kernel<SIX>);
         if (e != cudaSuccess) return e;
         e = one_wave(coop_rescue_kernel<SIX>, RL.bytes, cap, a.n_tasks, blocks, kCoopWarps * 32);
         if (e != cudaSuccess) return e;
-        coop_rescue_kernel<SIX><<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tmap, a, RL);
+        coop_rescue_kernel<SIX><<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tw_r > 0 ? tmap_r : tmap, a, RL);
         return cudaGetLastError();
     }
     e = allow_max_smem(solve_kernel<SIX, false>);
@@ -2384,6 +2372,21 @@ void tile_box(int dim, int six, int& tw, int& th) {
     if (tw > 256 || th > 256) tw = th = 0;
 }
 
+// The rescue pass's tile: twice the support each way (capped by the TMA box
+// limit), so the wide warps of Simplex probes and diverging iterations keep
+// reading shared memory; 0 when the fast pass's box is unavailable.
+void rescue_tile_box(int dim, int six, int& tw, int& th) {
+    int fw = 0, fh = 0;
+    tile_box(dim, six, fw, fh);
+    if (fw == 0) {
+        tw = th = 0;
+        return;
+    }
+    const int need = dim + (six ? 5 : 3) + 2;
+    tw = std::min(((2 * need + 7) + 3) & ~3, 256);
+    th = std::min(2 * need, 256);
+}
+
 cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStream_t st) {
     SolveArgs a = a0;
     CUtensorMap tmap;
@@ -2406,6 +2409,25 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     }
     a.tile_w = tw;
     a.tile_h = th;
+    CUtensorMap tmap_r;
+    std::memset(&tmap_r, 0, sizeof(tmap_r));
+    int tw_r = 0, th_r = 0;
+    if (tw > 0) {
+        rescue_tile_box(a.dim, six, tw_r, th_r);
+        const cuuint64_t gdim[2] = {(cuuint64_t)a.W, (cuuint64_t)a.H};
+        const cuuint64_t gstride[1] = {(cuuint64_t)a.pitch * 4};
+        const cuuint32_t box[2] = {(cuuint32_t)tw_r, (cuuint32_t)th_r};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = enc(&tmap_r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(a.defI), gdim, gstride,
+                               box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                               CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            // the rescue pass then uses the fast pass's box
+            tw_r = tw;
+            th_r = th;
+            tmap_r = tmap;
+        }
+    }
     const SmemLayout L = smem_layout(a.max_n, tw, th);
     a.smem_per_warp = L.bytes;
     a.half = a.dim / 2;
@@ -2436,8 +2458,8 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     // reference planes of another frame are read by the staged solver only
     const bool own_ref = (a.ref_pitch > 0 && a.ref_pitch != a.pitch) || a.ref_dx != 0 || a.ref_dy != 0;
     if (own_ref && !staged_ok) return cudaErrorInvalidValue;
-    return six ? launch_passes<true>(tmap, a, SL, staged_ok, grid_blocks, smem, st)
-               : launch_passes<false>(tmap, a, SL, staged_ok, grid_blocks, smem, st);
+    return six ? launch_passes<true>(tmap, tmap_r, tw_r, th_r, a, SL, staged_ok, grid_blocks, smem, st)
+               : launch_passes<false>(tmap, tmap_r, tw_r, th_r, a, SL, staged_ok, grid_blocks, smem, st);
 }
 
 }  // namespace dic
