@@ -1186,10 +1186,7 @@ struct WarpSolver {
 #pragma unroll
             for (int w = 1; w < kCoopWarps; ++w) g |= gbits[w * 32 + lane];
             valid = g & refok;
-            float part = 0.0f;
-#pragma unroll 4
-            for (int k = 0; k < K; ++k)
-                if ((valid >> k) & 1u) part = part + vals[lane + 32 * k];
+            const float part = vals_chain(valid, 0.0f, [](float v, float a) { return a + v; });
             sum = wsum(part);
             return wsum(__popcll((unsigned long long)valid));
         }
@@ -1356,13 +1353,40 @@ struct WarpSolver {
         return wsum(cnt);
     }
 
+    // COOP: this lane's ordered chain over vals, acc = f(vals[lane + 32 k],
+    // acc) for the valid pixels in increasing k, eight values loaded ahead of
+    // their eight steps so that the loads do not wait on the chain.
+    template <class F>
+    __device__ __forceinline__ float vals_chain(Mask valid, float acc, F&& f) const {
+#pragma unroll
+        for (int k0 = 0; k0 < K; k0 += 8) {
+            float v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int i = lane + 32 * (k0 + u);
+                v[u] = k0 + u < K ? vals[i < n ? i : n - 1] : 0.0f;
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                if (k0 + u < K && ((valid >> (k0 + u)) & 1u)) acc = f(v[u], acc);
+        }
+        return acc;
+    }
+
     __device__ __forceinline__ float sum_sq(float mean, Mask valid) const {
         float sq = 0.0f;
+        if constexpr (COOP) {
+            sq = vals_chain(valid, 0.0f, [&](float v, float a) {
+                const float d = v - mean;
+                return __fmaf_rn(d, d, a);
+            });
+        } else {
 #pragma unroll 4
-        for (int k = 0; k < K; ++k) {
-            if (!((valid >> k) & 1u)) continue;
-            const float d = vals[lane + 32 * k] - mean;
-            sq = __fmaf_rn(d, d, sq);
+            for (int k = 0; k < K; ++k) {
+                if (!((valid >> k) & 1u)) continue;
+                const float d = vals[lane + 32 * k] - mean;
+                sq = __fmaf_rn(d, d, sq);
+            }
         }
         return wsum(sq);
     }
@@ -1739,12 +1763,7 @@ struct WarpSolver {
             coop_post(5, nullptr);
             residual_part(0, min(K, per), valid, mean, inv, sdev, full);
             coop_bar();
-#pragma unroll 4
-            for (int k = 0; k < K; ++k) {
-                if (!((valid >> k) & 1u)) continue;
-                const float d = vals[lane + 32 * k];
-                ep = __fmaf_rn(d, d, ep);
-            }
+            ep = vals_chain(valid, 0.0f, [](float d, float a) { return __fmaf_rn(d, d, a); });
             const float score = wsum(ep) / (float)cnt;
             return finite_f(score) ? score : 2.0f;
         }
@@ -2142,14 +2161,18 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
 // coarse search's 256 offsets) is shared by all warps of the block. The
 // ordered reductions stay on warp 0, so the results are those of a single
 // warp. Every exit of the driver's loop posts "done", which is what ends the
-// other warps' loop.
-template <bool SIX>
+// other warps' loop. DIMC > 0: the subset size known at compile time (the
+// launch checks it), so warp 0's ordered per-lane chains unroll with their
+// loads ahead, and subsets of at most 1024 pixels use 32-bit validity masks.
+template <bool SIX, int DIMC>
 __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const __grid_constant__ CUtensorMap tmap,
                                                                          const SolveArgs a, const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
-    WarpSolver<SIX, uint64_t, true, true> s;
-    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, a.n, a.dim, a.pitch, L.tile_w,
-                 L.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+    using Mask = std::conditional_t<(DIMC > 0 && DIMC * DIMC <= 1024), uint32_t, uint64_t>;
+    WarpSolver<SIX, Mask, true, true> s;
+    solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
+                 DIMC > 0 ? DIMC : a.dim, a.pitch, L.tile_w, L.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch,
+                 a.ref_dx, a.ref_dy);
     if (s.warp != 0) {
         s.coop_serve();
         return;
@@ -2331,11 +2354,15 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const CUtensorMap& tmap_r, in
         // the rescue pass: a block of kCoopWarps warps per task, with its own
         // larger tile (one block per SM leaves the shared memory for it)
         const StagedLayout RL = staged_layout(a.n, tw_r, th_r, true, true);
-        e = allow_max_smem(coop_rescue_kernel<SIX>);
+        auto coop = coop_rescue_kernel<SIX, 0>;
+        if (a.dim == 21) coop = coop_rescue_kernel<SIX, 21>;
+        if (a.dim == 31) coop = coop_rescue_kernel<SIX, 31>;
+        if (a.dim == 41) coop = coop_rescue_kernel<SIX, 41>;
+        e = allow_max_smem(coop);
         if (e != cudaSuccess) return e;
-        e = one_wave(coop_rescue_kernel<SIX>, RL.bytes, cap, a.n_tasks, blocks, kCoopWarps * 32);
+        e = one_wave(coop, RL.bytes, cap, a.n_tasks, blocks, kCoopWarps * 32);
         if (e != cudaSuccess) return e;
-        coop_rescue_kernel<SIX><<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tw_r > 0 ? tmap_r : tmap, a, RL);
+        coop<<<(unsigned)blocks, kCoopWarps * 32, RL.bytes, st>>>(tw_r > 0 ? tmap_r : tmap, a, RL);
         return cudaGetLastError();
     }
     e = allow_max_smem(solve_kernel<SIX, false>);
