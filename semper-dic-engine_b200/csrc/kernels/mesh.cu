@@ -188,25 +188,40 @@ __global__ void path_a_tasks_kernel(int gw, int gh, int rect_x, int rect_y, int 
 __global__ void commit_kernel(const dic_task* __restrict__ tasks, const int* __restrict__ n_tasks,
                               const dic_result* __restrict__ res, FieldGrid f, PathStats* __restrict__ st) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= *n_tasks) return;
-    const dic_result r = res[t];
-    if (!(r.flags & DIC_RES_INITIALIZED)) return;
-    const int node = tasks[t].node;
-    atomicAdd(&st->icgn_iters, (unsigned long long)r.iters);
-    if (r.flags & DIC_RES_RESCUE) {
-        atomicAdd(&st->simp_calls, 1);
-        if (r.status == 0 && r.score <= 0.15f) atomicAdd(&st->simp_saved, 1);
-        else atomicAdd(&st->simp_dead, 1);
+    dic_result r{};
+    bool live = t < *n_tasks;
+    if (live) r = res[t];
+    live = live && (r.flags & DIC_RES_INITIALIZED);
+    const bool good = live && r.status == 0 && r.score <= 0.15f;
+    const bool rescued = live && (r.flags & DIC_RES_RESCUE);
+    if (live) {
+        const int node = tasks[t].node;
+        f.iters[node] = r.iters;
+        if (good) {
+            f.u[node] = r.u; f.v[node] = r.v; f.ux[node] = r.ux; f.uy[node] = r.uy;
+            f.vx[node] = r.vx; f.vy[node] = r.vy; f.corr[node] = r.score;
+            f.solved[node] = 1;
+        } else {
+            f.solved[node] = 0;
+            f.corr[node] = -1.0f;
+        }
     }
-    f.iters[node] = r.iters;
-    if (r.status == 0 && r.score <= 0.15f) {
-        f.u[node] = r.u; f.v[node] = r.v; f.ux[node] = r.ux; f.uy[node] = r.uy;
-        f.vx[node] = r.vx; f.vy[node] = r.vy; f.corr[node] = r.score;
-        f.solved[node] = 1;
-        atomicAdd(&st->points, 1);
-    } else {
-        f.solved[node] = 0;
-        f.corr[node] = -1.0f;
+    // the counts, summed over the warp first: one atomic per counter and warp
+    // instead of one per task on the same few addresses (integer sums, so the
+    // totals do not depend on the order)
+    const unsigned full = 0xffffffffu;
+    const unsigned iters = __reduce_add_sync(full, live ? (unsigned)r.iters : 0u);
+    const unsigned calls = __reduce_add_sync(full, rescued ? 1u : 0u);
+    const unsigned saved = __reduce_add_sync(full, rescued && good ? 1u : 0u);
+    const unsigned points = __reduce_add_sync(full, good ? 1u : 0u);
+    if ((threadIdx.x & 31) == 0) {
+        if (iters) atomicAdd(&st->icgn_iters, (unsigned long long)iters);
+        if (calls) {
+            atomicAdd(&st->simp_calls, (int)calls);
+            if (saved) atomicAdd(&st->simp_saved, (int)saved);
+            if (calls - saved) atomicAdd(&st->simp_dead, (int)(calls - saved));
+        }
+        if (points) atomicAdd(&st->points, (int)points);
     }
 }
 
