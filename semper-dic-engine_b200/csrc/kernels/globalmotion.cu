@@ -178,14 +178,21 @@ __global__ void cross_power_kernel(const float2* __restrict__ A, const float2* _
 }
 
 // argmax of the real part: value bits (positive floats order as integers)
-// packed above the index
+// packed above the index; the maximum over each warp first, then one atomic
+// per warp (the maximum does not depend on the order)
 __global__ void argmax_kernel(const float2* __restrict__ P, unsigned long long* best) {
     const size_t i = (size_t)blockIdx.y * N + blockIdx.x * blockDim.x + threadIdx.x;
-    if (blockIdx.x * blockDim.x + threadIdx.x >= N) return;
-    const float v = P[i].x;
-    if (!(v > 0.0f)) return;
-    const unsigned long long key = ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)i;
-    atomicMax(best, key);
+    unsigned long long key = 0;
+    if (blockIdx.x * blockDim.x + threadIdx.x < N) {
+        const float v = P[i].x;
+        if (v > 0.0f) key = ((unsigned long long)__float_as_uint(v) << 32) | (unsigned long long)i;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other > key ? other : key;
+    }
+    if ((threadIdx.x & 31) == 0 && key) atomicMax(best, key);
 }
 
 __global__ void neighbourhood_kernel(const float2* __restrict__ P, const unsigned long long* best,
