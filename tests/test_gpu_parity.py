@@ -309,3 +309,73 @@ def test_cancel_during_run():
     e.cancel()
     rc3, pts3, _ = e.run(j["dfm"], j["prm"], mask=j["mask"])
     assert rc3 == rc2 and np.array_equal(pts3, pts)
+
+
+def test_pipeline_cfg1_2048_bit_exact():
+    """cfg1's field and full solve settings (step 4, subset 31, window 31) on a
+    2048^2 frame: 259k grid nodes, bit for bit."""
+    ref, dfm, prm, _ = sb.config_pair(1, size=2048)
+    d, o = _run_both(ref, dfm, prm)
+    assert o[0] > 240000
+    _assert_field_equal(d, o)
+
+
+def test_pipeline_target_settings_2048_bit_exact():
+    """The target settings (step 8, subset 41, window 41) under the cfg1 field
+    on a 2048^2 frame, bit for bit."""
+    ref, dfm, prm, _ = sb.config_pair(4, size=2048)
+    d, o = _run_both(ref, dfm, prm)
+    assert o[0] > 55000
+    _assert_field_equal(d, o)
+
+
+def test_batch_cfg2_jobs_against_restatement():
+    """Eight pairs of the batched uneven workload (masks, rotations, subsets
+    15-41, steps 4 and 8), solved in one batch call, each against the CPU
+    restatement given the global model a lone device run estimates."""
+    jobs = sb.batch_jobs(8, seed=22, min_side=256, max_side=1024)
+    got = sb.Batch(workers=4).run(jobs)
+    positive = 0
+    for j, (rc, pts, met) in zip(jobs, got):
+        e = sb.Engine()
+        assert e.set_reference(j["ref"], j["mask"]) == 0
+        lrc, _, _ = e.run(j["dfm"], j["prm"], mask=j["mask"])
+        assert lrc == rc
+        g = e.last_global_motion()
+        o = oracle.Oracle(False)
+        o.set_reference(j["ref"], j["mask"])
+        p = j["prm"]
+        orc, opts, omet = o.run(j["dfm"], [p.rect_x, p.rect_y, p.rect_w, p.rect_h, p.step, p.subset_size,
+                                           p.strain_window, 0], mask=j["mask"],
+                                model_h=g["H"] if g["locked"] else None)
+        _assert_field_equal((rc, pts, met), (orc, opts, omet))
+        positive += rc > 0
+    assert positive >= 5 and sb.SEMPER_ERR_STRAIN_WINDOW in [g[0] for g in got]
+
+
+def test_tma_wait_that_runs_out_falls_back_bit_exact():
+    """The solve's TMA waits given a limit of one poll: the first tile copy of
+    (nearly) every warp is still in flight when its wait gives up, so the warp
+    samples global memory from then on, and waits for the late copy before it
+    exits. The run reports the timeout, and its field is the CPU restatement's,
+    bit for bit, as with the default limit."""
+    ref, dfm, prm, _ = sb.config_pair(1, size=512)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    rc0, pts0, met0 = e.run(dfm, prm)
+    assert e.last_tma_timeout() == 0
+    assert e.set_tma_wait_limit(1) == 0
+    rc1, pts1, met1 = e.run(dfm, prm)
+    assert e.last_tma_timeout() == 1
+    assert rc1 == rc0 > 10000
+    assert np.array_equal(pts1, pts0)
+    assert np.array_equal(met1[COUNT_SLOTS], met0[COUNT_SLOTS])
+    g = e.last_global_motion()
+    o = oracle.Oracle(False)
+    o.set_reference(ref)
+    p = [prm.rect_x, prm.rect_y, prm.rect_w, prm.rect_h, prm.step, prm.subset_size, prm.strain_window, 0]
+    orc, opts, _ = o.run(dfm, p, model_h=g["H"] if g["locked"] else None)
+    assert orc == rc1 and np.array_equal(pts1, opts)
+    assert e.set_tma_wait_limit(0) == 0
+    rc2, pts2, _ = e.run(dfm, prm)
+    assert e.last_tma_timeout() == 0 and np.array_equal(pts2, pts0)
