@@ -75,19 +75,14 @@ def _peaks():
     return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
 
 
-def _ncu_traffic():
-    """DRAM bytes per launch of the IC-GN solve kernel from the committed ncu
-    summary (profiles/), scaled to one cfg1 launch; None if not recorded."""
-    p = os.path.join(REPO, "profiles", "icgn_solve_cfg1.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.startswith("traffic_bytes_per_cfg1_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip())
-            except ValueError:
-                return None
-    return None
+# DRAM bytes per subset pixel-iteration of the IC-GN fast pass (the Path A
+# launch), from one `ncu --set full` capture per solve setting (summaries in
+# profiles/icgn_solve_cfg1.md and profiles/icgn_solve_cfg4.md): the cfg1 pair
+# at 2048x2048, step 4, subset 31 read 149.6 MB over 969,920,963
+# pixel-iterations; the target-settings pair at 2048x2048, step 8, subset 41
+# read 99.5 MB over 408,104,775. Traffic grows with the pixel-iterations, so a
+# launch's traffic is this figure times the launch's own pixel-iterations.
+NCU_BYTES_PER_PIXEL_ITER = {31: 149.6e6 / 969920963, 41: 99.5e6 / 408104775}
 
 
 class ClockSampler:
@@ -142,8 +137,8 @@ class ClockSampler:
 
 
 def cpu_sample(ref, dfm, prm, fp64=False, model=None):
-    """The CPU restatement on the central 1024 x 1024 ROI of the frame pair at
-    the same settings, reference cache warm (the solve timed is the second on
+    """The CPU restatement (built with the reference's compiler flags) on the
+    central 1024 x 1024 ROI of the frame pair at the same settings, reference cache warm (the solve timed is the second on
     the reference), given the global model the device used (None: none).
     Returns (points, seconds, attempted)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -153,7 +148,7 @@ def cpu_sample(ref, dfm, prm, fp64=False, model=None):
     side = min(1024, n)
     x0 = (n - side) // 2
     p = [x0, x0, side, side, prm.step, prm.subset_size, prm.strain_window, prm.use_6x6_interpolator]
-    o = oracle.Oracle(fp64)
+    o = oracle.Oracle(fp64, kind="contract" if fp64 else "reference_flags")
     o.set_reference(ref)
     o.run(dfm, p, model_h=model)  # frame 1: fills the grid scan + Hessian pool cache
     t0 = time.perf_counter()
@@ -195,19 +190,28 @@ def accuracy_sample(eng, ref, dfm, prm, warp, p, gm):
             "vs_true_field_rms_px": float(np.sqrt(np.mean(t ** 2))), "vs_true_field_max_px": float(t.max())}
 
 
+REF_SAMPLE_SIDE = 1024
+
+
 def run_reference(args, rank):
+    """The reference arm: the CPU restatement built with the reference's own
+    compiler flags, on every host thread, on the central 1024x1024 ROI of the
+    headline pair (about 62 k points a step; the full 4096x4096 frame takes
+    about 25 s a step on the CPU). Its inputs come from the checker's own build
+    of the speckle generator: this arm loads no library of the package."""
     if rank != 0:
         return 0
-    import semper_b200 as sb
-
-    ref, dfm, prm, _ = sb.config_pair(1)
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
 
-    side = 1024
+    import semper_b200 as sb
+
+    sb.use_synth_library(oracle.synth_path())
+    ref, dfm, prm, _ = sb.config_pair(1)
+    side = REF_SAMPLE_SIDE
     x0 = (ref.shape[0] - side) // 2
     p = [x0, x0, side, side, prm.step, prm.subset_size, prm.strain_window, 0]
-    o = oracle.Oracle(False)
+    o = oracle.Oracle(False, kind="reference_flags")
     o.set_reference(ref)
     for _ in range(max(args.warmup, 1)):
         o.run(dfm, p)
@@ -218,15 +222,17 @@ def run_reference(args, rank):
         t_total += time.perf_counter() - t0
         pts_total += rc
     v = pts_total / t_total
-    cores = os.cpu_count()
+    cores = len(os.sched_getaffinity(0))
+    sample = (f"central {side}x{side} ROI ({p[2] // p[4]}^2 grid) of the cfg1 4096x4096 pair, reference cache "
+              f"warm, no global model; CPU restatement built with the reference's flags (-O3 -ffast-math "
+              f"-fno-finite-math-only -ffp-contract=off), OpenMP on {cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample": f"central {side}x{side} ROI of the 4096x4096 pair"},
-        "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
-                         "sample": f"central {side}x{side} ROI ({p[2] // p[4]}^2 grid) of the cfg1 pair, "
-                                   f"reference cache warm"},
+        "config": {"workload": WORKLOAD, "sample": sample, "same_config": False,
+                   "differs_by": "a 1024x1024 ROI of the same pair and settings instead of the whole frame"},
+        "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -248,25 +254,18 @@ def aggregate(points, ms_per_step, steps, dist=None, device="cpu"):
     return float(pts_t.item()) / steps / (ms_max / 1000.0), ms_max
 
 
-def run_b200(args, rank, world, local_rank):
+def measure_frames(args, wl, rank, world, local_rank, dist):
+    """Times one workload's frames on this rank: device-resident runs (value),
+    then the public C ABI from pinned host memory (e2e). Returns the pieces of
+    the JSON line; the CPU-baseline and accuracy legs run on rank 0 at N=1."""
     import torch
 
     import semper_b200 as sb
 
-    torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    workload = WORKLOADS[args.workload]
-    if args.workload == "cfg4-large":
+    if wl == "cfg4-large":
         ref, dfm, prm, warp, _sim = sb.large_motion_pair(args.size, pair=rank)
     else:
-        ref, dfm, prm, warp = sb.config_pair(4 if args.workload == "cfg4-plain" else 1, size=args.size, pair=rank)
+        ref, dfm, prm, warp = sb.config_pair(4 if wl == "cfg4-plain" else 1, size=args.size, pair=rank)
     H, W = ref.shape
     grid_nodes = (prm.rect_w // prm.step) * (prm.rect_h // prm.step)
     capacity = grid_nodes * 8
@@ -328,64 +327,90 @@ def run_b200(args, rank, world, local_rank):
     e2e_value = rc_e2e * world / (float(e2e_t.item()) / 1000.0)
 
     # roofline of the IC-GN solve kernel (Path A launch)
+    six = bool(prm.use_6x6_interpolator)
     a_ms = statistics.mean(p["path_a"] for p in phases)
     a_pix = statistics.mean(c["path_a_pixel_iters"] for c in counts)
-    flops = FLOP_PER_PIXEL_ITER[bool(prm.use_6x6_interpolator)] * a_pix
+    flops = FLOP_PER_PIXEL_ITER[six] * a_pix
     achieved = flops / (a_ms / 1000.0) / 1e12
     peaks, peak_src = _peaks()
     sms = torch.cuda.get_device_properties(local_rank).multi_processor_count
     fp32_peak = sms * 128 * 2 * float(peaks.get("sm_max_mhz", 1965.0)) * 1e6 / 1e12
-    traffic = _ncu_traffic()
-    clocks = clk.summary()
+    bpp = NCU_BYTES_PER_PIXEL_ITER.get(prm.subset_size) if not six else None
+    traffic = None if bpp is None else bpp * a_pix
     gm = eng.last_global_motion()
 
-    line = None
+    out = {
+        "value": value, "ms_per_step": ms_max,
+        "config": {"workload": WORKLOADS[wl] if args.size == 4096 else f"{WORKLOADS[wl]} [resized to {W}x{H}]",
+                   "image": [W, H], "grid_nodes": grid_nodes,
+                   "attempted": int(met[0]), "points_per_step": rc,
+                   "parallelism": f"replicas x{world} (independent frame pairs)",
+                   "l2": f"inputs larger than L2: reference planes {12 * W * H / 1e6:.0f} MB + Hessian pool "
+                         f"{177 * grid_nodes / 1e6:.0f} MB + deformed planes {12 * W * H / 1e6:.0f} MB per step"},
+        "frames_per_s": 1000.0 / ms_max * world,
+        "attempted_points_per_s": int(met[0]) * world / (ms_max / 1000.0),
+        "first_frame_ms": round(first_ms, 2),
+        "first_frame_pool_ms": round(first_t["pool"], 3),
+        "phases_ms": {k: round(statistics.mean(p[k] for p in phases), 3) for k in phases[0]},
+        "mean_icgn_iters_per_point": float(met[8]),
+        "fast_pass_shape": {0: "reference from the planes", 1: "reference staged", -1: "undecided"}[
+            eng.fast_pass_shape(prm.subset_size, six)],
+        "global_model": {"locked": gm["locked"], "rotation_deg": float(np.degrees(gm["theta"])),
+                         "scale": gm["scale"], "translation_px": [float(gm["t"][0]), float(gm["t"][1])]},
+        "e2e": {"value": e2e_value, "unit": "points/s",
+                "h2d_bytes_per_step": int(W * H), "d2h_bytes_per_step": int(rc_e2e * 32)},
+        "roofline": {"kernel": "icgn solve (Path A launch)", "bound": "fp32", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": traffic,
+                     "traffic_source": None if traffic is None else
+                     f"ncu DRAM bytes per pixel-iteration of a 2048x2048 capture at subset {prm.subset_size} "
+                     f"x {int(a_pix)} pixel-iterations",
+                     "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 x {peaks.get('sm_max_mhz', 1965.0)} MHz "
+                                    f"({peak_src} sm_max_mhz)",
+                     "algorithmic": f"{FLOP_PER_PIXEL_ITER[six]} FLOP per subset pixel per iteration x "
+                                    f"{int(a_pix)} pixel-iterations per launch"},
+        "clocks": clk.summary(),
+        "gpu_launches": int(sum(c["launches"] for c in counts)),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm, model=gm["H"] if gm["locked"] else None)
+        out["cpu_baseline"] = {"value": crc / cdt, "unit": "points/s", "cores": len(os.sched_getaffinity(0)),
+                               "kind": "port",
+                               "sample": f"central {cp[2]}x{cp[3]} ROI ({cp[2] // cp[4]}^2 grid, {catt} attempted) "
+                                         f"of the same pair, reference cache warm, {cdt:.2f} s"}
+        out["accuracy"] = accuracy_sample(eng, ref, dfm, prm, warp, cp, gm)
+    eng.close()
+    return out
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    m = measure_frames(args, args.workload, rank, world, local_rank, dist)
+    # The default line also measures the target settings (4096^2, step 8,
+    # subset 41 under the same field), where the task states its speed-up and
+    # roofline targets; every rank takes the same steps.
+    tgt = None
+    if args.workload == "cfg1" and not args.no_target:
+        tgt = measure_frames(args, "cfg4-plain", rank, world, local_rank, dist)
     if rank == 0:
-        cpu = None
-        accuracy = None
-        if world == 1 and not args.no_cpu:
-            crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm, model=gm["H"] if gm["locked"] else None)
-            cpu = {"value": crc / cdt, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
-                   "sample": f"central {cp[2]}x{cp[3]} ROI ({cp[2] // cp[4]}^2 grid, {catt} attempted) of the "
-                             f"same pair, reference cache warm, {cdt:.2f} s"}
-            accuracy = accuracy_sample(eng, ref, dfm, prm, warp, cp, gm)
-        mean_phase = {k: round(statistics.mean(p[k] for p in phases), 3) for k in phases[0]}
-        line = {
-            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload if args.size == 4096 else f"{workload} [resized to {W}x{H}]",
-                       "image": [W, H], "grid_nodes": grid_nodes,
-                       "attempted": int(met[0]), "points_per_step": rc,
-                       "parallelism": f"replicas x{world} (independent frame pairs)",
-                       "l2": f"inputs larger than L2: reference planes {12 * W * H / 1e6:.0f} MB + Hessian pool "
-                             f"{177 * grid_nodes / 1e6:.0f} MB + deformed planes {12 * W * H / 1e6:.0f} MB per step"},
-            "frames_per_s": 1000.0 / ms_max * world,
-            "attempted_points_per_s": int(met[0]) * world / (ms_max / 1000.0),
-            "first_frame_ms": round(first_ms, 2),
-            "first_frame_pool_ms": round(first_t["pool"], 3),
-            "phases_ms": mean_phase,
-            "mean_icgn_iters_per_point": float(met[8]),
-            "fast_pass_shape": {0: "reference from the planes", 1: "reference staged", -1: "undecided"}[
-                eng.fast_pass_shape(prm.subset_size, bool(prm.use_6x6_interpolator))],
-            "global_model": {"locked": gm["locked"], "rotation_deg": float(np.degrees(gm["theta"])),
-                             "scale": gm["scale"], "translation_px": [float(gm["t"][0]), float(gm["t"][1])]},
-            "e2e": {"value": e2e_value, "unit": "points/s",
-                    "h2d_bytes_per_step": int(W * H), "d2h_bytes_per_step": int(rc_e2e * 32)},
-            "roofline": {"kernel": "icgn solve (Path A launch)", "bound": "fp32", "achieved": achieved,
-                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                         "traffic": traffic,
-                         "peak_source": f"{sms} SMs x 128 FP32 lanes x 2 x {peaks.get('sm_max_mhz', 1965.0)} MHz "
-                                        f"({peak_src} sm_max_mhz)",
-                         "algorithmic": f"{FLOP_PER_PIXEL_ITER[False]} FLOP per subset pixel per iteration x "
-                                        f"{int(a_pix)} pixel-iterations per launch"},
-            "clocks": clocks,
-            "gpu_launches": int(sum(c["launches"] for c in counts)),
-        }
-        if cpu:
-            line["cpu_baseline"] = cpu
-        if accuracy:
-            line["accuracy"] = accuracy
+        line = {"metric": METRIC, "value": m["value"], "unit": "points/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic"}
+        line.update({k: v for k, v in m.items() if k not in ("value", "ms_per_step")})
+        if tgt is not None:
+            t = {"value": tgt["value"], "unit": "points/s", "ms_per_step": tgt["ms_per_step"]}
+            t.update({k: v for k, v in tgt.items() if k not in ("value", "ms_per_step")})
+            line["target_settings"] = t
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
@@ -507,7 +532,7 @@ def run_cfg2(args, rank):
         small = sorted(jobs, key=lambda j: j["ref"].size)[: max(1, args.pairs // 16)]
         cpts, cdt = 0, 0.0
         for j in small:
-            o = oracle.Oracle(False)
+            o = oracle.Oracle(False, kind="reference_flags")
             o.set_reference(j["ref"], j["mask"])
             p = [0, 0, j["ref"].shape[1], j["ref"].shape[0], j["prm"].step, j["prm"].subset_size,
                  j["prm"].strain_window, 0]
@@ -515,7 +540,8 @@ def run_cfg2(args, rank):
             rc, _, _ = o.run(j["dfm"], p, mask=j["mask"])
             cdt += time.perf_counter() - t0
             cpts += max(rc, 0)
-        line["cpu_baseline"] = {"value": cpts / cdt, "unit": "points/s", "cores": os.cpu_count(), "kind": "port",
+        line["cpu_baseline"] = {"value": cpts / cdt, "unit": "points/s", "cores": len(os.sched_getaffinity(0)),
+                                "kind": "port",
                                 "sample": f"the {len(small)} smallest pairs, one cold solve each, {cdt:.1f} s"}
     print(json.dumps(line), flush=True)
     return 0
@@ -528,6 +554,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-target", action="store_true",
+                    help="cfg1 only: skip the nested target-settings measurement (step 8, subset 41)")
     ap.add_argument("--size", type=int, default=4096,
                     help="image edge (default 4096, the benchmark workload; smaller sizes are for profiling)")
     ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg4-plain", "cfg4-large", "cfg3"],

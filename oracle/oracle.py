@@ -14,7 +14,12 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+# The same restatement built with the reference's own compiler flags: timed as
+# the CPU baseline, never used to check results bit for bit.
+_REFFLAGS_PATH = os.path.join(_HERE, "_build", "liboracle_refflags.so")
+_SYNTH_PATH = os.path.join(_HERE, "_build", "liboracle_synth.so")
 _lib = None
+_libs = {}
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
 _i32p = ctypes.POINTER(ctypes.c_int32)
@@ -28,12 +33,19 @@ def build() -> str:
     return _LIB_PATH
 
 
-def lib():
+def lib(kind: str = "contract"):
+    """The restatement library: kind "contract" (the checker, strict IEEE
+    arithmetic mirroring the device) or "reference_flags" (the timing build)."""
     global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+    if kind == "contract" and _lib is not None:
+        return _lib
+    if kind in _libs:
+        return _libs[kind]
+    path = {"contract": _LIB_PATH, "reference_flags": _REFFLAGS_PATH}[kind]
+    if True:
+        if not os.path.exists(path):
             build()
-        L = ctypes.CDLL(_LIB_PATH)
+        L = ctypes.CDLL(path)
         L.oracle_create.restype = ctypes.c_void_p
         L.oracle_create.argtypes = [ctypes.c_int]
         L.oracle_destroy.argtypes = [ctypes.c_void_p]
@@ -66,8 +78,19 @@ def lib():
             [_f32p, _f32p, _u8p, ctypes.c_int, _u8p]
         L.oracle_inc_match.argtypes = [_u8p, _u8p, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                        ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
-        _lib = L
-    return _lib
+        _libs[kind] = L
+        if kind == "contract":
+            _lib = L
+    return L
+
+
+def synth_path() -> str:
+    """Path of the oracle-side build of the seeded speckle generator (the same
+    C ABI as the package's synth library), for a CPU-only caller that loads no
+    library of the package."""
+    if not os.path.exists(_SYNTH_PATH):
+        build()
+    return _SYNTH_PATH
 
 
 def _p(a, t):
@@ -77,12 +100,13 @@ def _p(a, t):
 class Oracle:
     """One reference cache (ReferenceCache) of the restatement."""
 
-    def __init__(self, fp64: bool = False):
-        self._h = lib().oracle_create(1 if fp64 else 0)
+    def __init__(self, fp64: bool = False, kind: str = "contract"):
+        self._L = lib(kind)
+        self._h = self._L.oracle_create(1 if fp64 else 0)
 
     def close(self):
-        if self._h:
-            lib().oracle_destroy(self._h)
+        if getattr(self, "_h", None):
+            self._L.oracle_destroy(self._h)
             self._h = None
 
     __del__ = close
@@ -90,7 +114,7 @@ class Oracle:
     def set_reference(self, gray: np.ndarray, mask: np.ndarray | None = None) -> int:
         gray = np.ascontiguousarray(gray, np.uint8)
         m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
-        return lib().oracle_set_reference(self._h, _p(gray, _u8p), gray.shape[1], gray.shape[0], _p(m, _u8p))
+        return self._L.oracle_set_reference(self._h, _p(gray, _u8p), gray.shape[1], gray.shape[0], _p(m, _u8p))
 
     def run(self, deformed: np.ndarray, params, capacity: int | None = None, mask=None, model_h=None,
             metrics_len: int = 24, capture: bool = False):
@@ -104,14 +128,14 @@ class Oracle:
         met = np.zeros(max(metrics_len, 1), np.float32)
         H = None if model_h is None else np.ascontiguousarray(model_h, np.float64).reshape(9)
         if not capture:
-            rc = lib().oracle_run(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
+            rc = self._L.oracle_run(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
                                   capacity, _p(met, _f32p), metrics_len, _p(H, _f64p))
             pts = out[: max(rc, 0) * 8].reshape(-1, 8).copy()
             return rc, pts, met[:metrics_len].copy()
         n = int(gw * gh) + 16
         gf = np.zeros((n, 7), np.float32)
         gi = np.zeros((n, 4), np.int32)
-        rc = lib().oracle_run_capture(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
+        rc = self._L.oracle_run_capture(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
                                       capacity, _p(met, _f32p), metrics_len, _p(H, _f64p),
                                       _p(gf, _f32p), _p(gi, _i32p), n)
         pts = out[: max(rc, 0) * 8].reshape(-1, 8).copy()

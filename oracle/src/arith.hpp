@@ -18,8 +18,18 @@ namespace oracle {
 
 constexpr int kLanes = 32;
 
+#ifdef ORACLE_REFERENCE_FLAGS
+// The timing build (the CPU baseline), compiled with the reference's own flags
+// (CMakeLists.txt:80: -O3 -ffast-math -fno-finite-math-only -ffp-contract=off):
+// every multiply-add is a separate multiply and add, as the reference computes
+// it, not a library fma call on a target without the instruction. Its bits
+// differ from the device contract; it is timed, never compared bit for bit.
+inline float fmaT(float a, float b, float c) { return a * b + c; }
+inline double fmaT(double a, double b, double c) { return a * b + c; }
+#else
 inline float fmaT(float a, float b, float c) { return std::fmaf(a, b, c); }
 inline double fmaT(double a, double b, double c) { return std::fma(a, b, c); }
+#endif
 
 // Warp xor-butterfly: after the step with offset o, lane l holds
 // v[l] + v[l ^ o]. IEEE addition is commutative, so every lane ends with the

@@ -187,7 +187,7 @@ PoolEntry<T> compute_hessian_only(const Image<T>& im, int cx, int cy, int dim) {
                              (double)(g1 * fx), (double)(g1 * fy)};
         int q = 0;
         for (int r = 0; r < 6; ++r)
-            for (int c = r; c < 6; ++c, ++q) hp[q][i % kLanes] = fma(s[r], s[c], hp[q][i % kLanes]);
+            for (int c = r; c < 6; ++c, ++q) hp[q][i % kLanes] = fmaT(s[r], s[c], hp[q][i % kLanes]);
     }
     int q = 0;
     for (int r = 0; r < 6; ++r)
@@ -372,7 +372,7 @@ struct Engine {
                     int q = 0;
                     for (int r = 0; r < 6; ++r)
                         for (int c = r; c < 6; ++c, ++q)
-                            hp[q][l] = fma((double)sp[r], (double)sp[c], hp[q][l]);
+                            hp[q][l] = fmaT((double)sp[r], (double)sp[c], hp[q][l]);
                 }
             }
             const T err = butterfly(ep);
@@ -402,7 +402,7 @@ struct Engine {
             T dp[6];
             for (int r = 0; r < 6; ++r) {
                 double a = 0.0;
-                for (int c = 0; c < 6; ++c) a = fma(Hstep[r][c], (double)g[c], a);
+                for (int c = 0; c < 6; ++c) a = fmaT(Hstep[r][c], (double)g[c], a);
                 dp[r] = (T)(-a);
             }
             // dW = I + [[dp2, dp3, dp0], [dp4, dp5, dp1]]; W <- W dW^-1

@@ -38,7 +38,8 @@ C_SYMBOLS = ["semper_cancel", "semper_create", "semper_destroy", "semper_increme
 EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b200_set_global_model",
                "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion",
                "semper_b200_batch_create", "semper_b200_batch_destroy", "semper_b200_batch_run",
-               "semper_b200_batch_last_error", "semper_b200_incremental_profile", "semper_b200_fast_pass_shape"]
+               "semper_b200_batch_last_error", "semper_b200_incremental_profile", "semper_b200_fast_pass_shape",
+               "semper_b200_set_tma_wait_limit", "semper_b200_last_tma_timeout"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -106,6 +107,8 @@ def lib():
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
         L.semper_b200_fast_pass_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
         L.semper_b200_set_global_motion.argtypes = [_vp, ctypes.c_int]
+        L.semper_b200_set_tma_wait_limit.argtypes = [_vp, ctypes.c_int]
+        L.semper_b200_last_tma_timeout.argtypes = [_vp]
         L.semper_b200_batch_create.argtypes = [ctypes.c_int32]
         L.semper_b200_batch_create.restype = _vp
         L.semper_b200_batch_destroy.argtypes = [_vp]
@@ -129,6 +132,15 @@ def lib():
         L.dic_cuda_pack.argtypes = [ctypes.c_int] * 6 + [_vp] * 9 + [ctypes.c_size_t, _vp]
         _lib = L
     return _lib
+
+
+def use_synth_library(path: str) -> None:
+    """Generate speckle with another build of the same generator (same C ABI),
+    e.g. the checker's own copy for a CPU-only caller; before the first use."""
+    global SYNTH_PATH, _synth
+    if _synth is not None:
+        raise RuntimeError("the speckle generator is already loaded")
+    SYNTH_PATH = path
 
 
 def synth_lib():
@@ -222,6 +234,12 @@ class Engine:
     def set_global_model(self, H=None) -> int:
         Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
         return lib().semper_b200_set_global_model(self._h, _p(Hm, _f64p))
+
+    def set_tma_wait_limit(self, polls: int) -> int:
+        return lib().semper_b200_set_tma_wait_limit(self._h, polls)
+
+    def last_tma_timeout(self) -> int:
+        return lib().semper_b200_last_tma_timeout(self._h)
 
     def set_global_motion(self, on: bool) -> int:
         return lib().semper_b200_set_global_motion(self._h, 1 if on else 0)

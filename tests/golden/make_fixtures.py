@@ -2,7 +2,8 @@
 
 Run here, where the reference checkout and OpenCV's Python module exist:
 
-    python tests/golden/make_fixtures.py [/path/to/reference]
+    python tests/golden/make_fixtures.py /path/to/reference
+    SEMPER_REFERENCE=/path/to/reference python tests/golden/make_fixtures.py
 
 It writes
   golden_corpus_bicubic.npz, golden_corpus_keys6x6.npz
@@ -132,4 +133,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SEMPER_REFERENCE")
+    if not root:
+        sys.exit("usage: make_fixtures.py <reference checkout>  (or set SEMPER_REFERENCE)")
+    main(root)
