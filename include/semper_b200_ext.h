@@ -49,6 +49,18 @@ SEMPER_C_API int semper_b200_fast_pass_shape(semper_engine* eng, int subset_size
    gives them ([8..15]). For measurement. Returns 0, or -3 for a NULL handle. */
 SEMPER_C_API int semper_b200_incremental_profile(semper_incremental* inc, double out[16]);
 
+/* The solve's bounded waits for its TMA tile copies: at most `polls` polls
+   of the copy's mbarrier (0: the default, about 0.1 s) before a wait gives
+   up. A warp whose wait ran out reads the deformed image from global memory
+   instead, with identical arithmetic and results, and waits (bounded) for the
+   late copy before it exits. A small limit exercises that path. Returns 0, or
+   -3 for a NULL or busy handle. */
+SEMPER_C_API int semper_b200_set_tma_wait_limit(semper_engine* eng, int polls);
+
+/* 1 when a TMA wait of the last run on this handle ran out, else 0; -3 for a
+   NULL handle. */
+SEMPER_C_API int semper_b200_last_tma_timeout(semper_engine* eng);
+
 /* A global-motion model for the following runs on this handle: a 3x3
    homography, reference -> deformed, row-major (the role of the reference's
    AKAZE front end, src/pipeline/full_field_anchors.cpp:204-279). NULL clears

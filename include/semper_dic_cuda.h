@@ -72,12 +72,17 @@ size_t dic_cuda_solve_scratch_bytes(int n_tasks);
    application's memory pool, a process under a fixed device-memory budget,
    code that must not call cudaMalloc mid-run). Same solve, arguments and
    results as dic_cuda_solve, without d_scratch: the scratch is a fixed array
-   in the library's device image (4 MiB per GPU that loads the library, held
-   until exit), so the call allocates nothing.
+   in the library's device image, so the call allocates nothing. The array
+   takes 4 MiB on a GPU once the library's device code is loaded there (with
+   CUDA's default lazy module loading, at the first use on that device) and
+   is held until exit.
    - n_tasks above DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS returns
      cudaErrorInvalidValue (1) and launches nothing.
    - The first call on a device looks up the array's device address with that
-     device current; make that first call before any stream capture.
+     device current and keeps it for later calls; make that first call before
+     any stream capture. The kept address does not survive a reset of the
+     device's primary context (cudaDeviceReset): do not use this entry across
+     one.
    - Every call shares the one array (the counters are zeroed on `stream` at
      the start of each call): calls whose work overlaps on the GPU, on
      different streams or from different threads, race and must be

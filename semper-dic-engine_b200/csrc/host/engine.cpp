@@ -371,6 +371,7 @@ struct Engine::Impl {
         a.H = E.H_;
         a.pitch = pitch();
         a.err = counters.p + 9;
+        a.tma_max_polls = E.tma_polls_;
         a.pool_valid = pool_valid.p;
         a.pool_ms = pool_ms.p;
         a.pool_Hs = pool_Hs.p;
@@ -446,10 +447,12 @@ struct Engine::Impl {
         launched(4, dic::launch_pack(gW, gH, rect_x, rect_y, step, max_pts, valid.p, fu.p, fv.p, fcorr.p, exx.p, eyy.p,
                                      exy.p, d_out_p, counters.p + 4, counters.p + 5, pack_scratch.p, pack_scratch.n, st),
                  "pack");
-        int cnts[3] = {0, 0, 0};
-        check(cudaMemcpyAsync(cnts, counters.p + 4, 3 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H pack");
+        // the packing counts [4..6] and, in the same copy, the run's TMA-wait flag [9]
+        int cnts[6] = {0, 0, 0, 0, 0, 0};
+        check(cudaMemcpyAsync(cnts, counters.p + 4, 6 * sizeof(int), cudaMemcpyDeviceToHost, st), "D2H pack");
         check(cudaEventRecord(ev[8], st), "event");
         sync();
+        E.last_tma_timeout_ = cnts[5];
         dropped_post = cnts[0];
         return std::min(cnts[1] + cnts[2], max_pts);
     }
@@ -751,6 +754,8 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
     try {
         poll_cancel();
         check(cudaEventRecord(ev[0], st), "event");
+        check(cudaMemsetAsync(counters.p + 9, 0, sizeof(int), st), "memset");
+        E.last_tma_timeout_ = 0;
         prepare_deformed(d_def);
         check(cudaEventRecord(ev[1], st), "event");
 

@@ -173,6 +173,12 @@ public:
     int fast_pass_shape(int subset_size, bool six) const;
     // Grid blocks of the persistent solve kernel (0: automatic).
     void set_solve_blocks(int b) { solve_blocks_ = b; }
+    // Polls of the solve's bounded TMA completion waits (0: the default,
+    // about 0.1 s). A wait that runs out makes that warp read global memory,
+    // with the same results; a small limit makes that path run.
+    void set_tma_wait_limit(int polls) { tma_polls_ = polls > 0 ? polls : 0; }
+    // Whether a TMA wait of the last run ran out (1) or not (0).
+    int last_tma_timeout() const { return last_tma_timeout_; }
 
     struct Impl;
 
@@ -184,6 +190,8 @@ private:
     bool has_ref_ = false;
     int W_ = 0, H_ = 0;
     int solve_blocks_ = 0;
+    int tma_polls_ = 0;
+    int last_tma_timeout_ = 0;
     bool global_motion_ = true;
     dic::GlobalSimilarity last_global_;
     PhaseTimes times_;

@@ -253,6 +253,19 @@ SEMPER_C_API int semper_b200_set_global_model(semper_engine* eng, const double* 
     return 0;
 }
 
+SEMPER_C_API int semper_b200_set_tma_wait_limit(semper_engine* eng, int polls) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    eng->engine.set_tma_wait_limit(polls);
+    return 0;
+}
+
+SEMPER_C_API int semper_b200_last_tma_timeout(semper_engine* eng) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    return eng->engine.last_tma_timeout();
+}
+
 SEMPER_C_API int semper_b200_set_global_motion(semper_engine* eng, int on) {
     if (eng == nullptr) return SEMPER_ERR_INIT;
     HandleCall call(eng->busy);

@@ -60,6 +60,11 @@ constexpr int kIcgnMaxIter = 50;
 constexpr float kGhostRejectFraction = 0.05f;
 constexpr float kGhost = -5.0f;
 constexpr int kCancelPollTasks = 32;  // a power of two
+// Polls of an mbarrier before a TMA completion wait gives up (about 0.1 s),
+// unless the launch asks for fewer. A wait that gives up sets the error flag
+// and the warp reads global memory from then on; before it exits, the warp
+// waits (bounded the same way) for the copy still in flight into its tile.
+constexpr int kTmaPolls = 1 << 22;
 
 struct Res {
     float u, v, ux, uy, vx, vy, score;
@@ -72,6 +77,8 @@ struct TileState {
     int ok;          // the tile holds the box at (tx0, ty0)
     int on;          // staging enabled (off after a wait ran out)
     unsigned phase;  // parity of the next barrier phase
+    int pend;        // a wait ran out: the copy of parity pend_phase may still be in flight
+    unsigned pend_phase;
 };
 
 // The per-subset values of a solve. Launch constants (plane pointers, image
@@ -182,7 +189,8 @@ __device__ __forceinline__ void ensure_tile(const Ctx& c, const float W[6]) {
         mbar_arrive_expect_tx(bar_of(c), (uint32_t)(c.a->tile_w * c.a->tile_h * 4));
         tma_load_2d(tile_of(c), c.tmap, nx, ny, bar_of(c));
     }
-    const bool done = __all_sync(kFull, mbar_wait_bounded(bar_of(c), phase, 1 << 22));
+    const int polls = c.a->tma_max_polls > 0 ? c.a->tma_max_polls : kTmaPolls;
+    const bool done = __all_sync(kFull, mbar_wait_bounded(bar_of(c), phase, polls));
     if (c.lane == 0) {
         ts->phase = phase ^ 1u;
         if (done) {
@@ -190,9 +198,11 @@ __device__ __forceinline__ void ensure_tile(const Ctx& c, const float W[6]) {
             ts->ty0 = ny;
             ts->ok = 1;
         } else {
-            // a copy that never completed: stop staging for this warp
+            // a copy that has not completed: stop staging for this warp
             ts->ok = 0;
             ts->on = 0;
+            ts->pend = 1;
+            ts->pend_phase = phase;
             if (c.a->err) atomicExch(c.a->err, 1);
         }
     }
@@ -636,6 +646,8 @@ __global__ void __launch_bounds__(32, 1)
         ts->ok = 0;
         ts->on = a.tile_w > 0 ? 1 : 0;
         ts->phase = 0;
+        ts->pend = 0;
+        ts->pend_phase = 0;
     }
     fence_proxy_async_smem();
     __syncwarp();
@@ -767,6 +779,11 @@ __global__ void __launch_bounds__(32, 1)
         }
         __syncwarp();
     }
+    // a copy whose wait ran out may still be writing into the tile: let it
+    // land (bounded) before the block's shared memory is released
+    const TileState* ts = reinterpret_cast<const TileState*>(my + 16);
+    __syncwarp();
+    if (ts->pend) (void)__all_sync(kFull, mbar_wait_bounded(reinterpret_cast<uint64_t*>(my), ts->pend_phase, kTmaPolls));
 }
 
 // ---------------------------------------------------------------------------
@@ -1056,18 +1073,33 @@ struct WarpSolver {
             mbar_arrive_expect_tx(bar, (uint32_t)(tw * th * 4));
             tma_load_2d(tile, tmap, nx, ny, bar);
         }
-        const bool done = __all_sync(kFull, mbar_wait_bounded(bar, phase, 1 << 22));
-        phase ^= 1u;
+        int* const aux = reinterpret_cast<int*>(bar + 1);  // [max polls, pending, pending parity]
+        const bool done = __all_sync(kFull, mbar_wait_bounded(bar, phase, aux[0]));
         if (done) {
             tx0 = nx;
             ty0 = ny;
             tile_ok = true;
         } else {
-            // a copy that never completed: stop staging for this warp
+            // a copy that has not completed: stop staging for this warp
             tile_ok = false;
             tile_on = false;
-            if (lane == 0 && err) atomicExch(err, 1);
+            if (lane == 0) {
+                aux[1] = 1;
+                aux[2] = (int)phase;
+                if (err) atomicExch(err, 1);
+            }
+            __syncwarp();
         }
+        phase ^= 1u;
+    }
+
+    // Before the warp exits: a copy whose wait ran out may still be writing
+    // into the tile; wait for it (bounded) so that it lands before the block's
+    // shared memory is released.
+    __device__ __forceinline__ void drain() {
+        const int* const aux = reinterpret_cast<const int*>(bar + 1);
+        __syncwarp();
+        if (aux[1]) (void)__all_sync(kFull, mbar_wait_bounded(bar, (unsigned)aux[2], kTmaPolls));
     }
 
     // The pixels k in [k_lo, k_hi) of this lane (i = lane + 32 k): their
@@ -2001,7 +2033,7 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
                                              const CUtensorMap* tmap, const float* refI, const float* refGx,
                                              const float* refGy, const float* defI, int* err, int n, int dim,
                                              int pitch, int tw, int th, int W, int H, int min_valid, int lm,
-                                             int ref_pitch, int ref_dx, int ref_dy) {
+                                             int ref_pitch, int ref_dx, int ref_dy, int max_polls) {
     const int lane = threadIdx.x & 31;
     s.bar = reinterpret_cast<uint64_t*>(smem);
     s.Hr = reinterpret_cast<double*>(smem + 64);
@@ -2053,8 +2085,15 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
     s.mflags = reinterpret_cast<int*>(smem + L.off_coop + kCoopFlags);
     s.scr_cond = reinterpret_cast<double*>(smem + L.off_coop + kCoopScrCond);
     s.scr_inv = reinterpret_cast<double*>(smem + L.off_coop + kCoopScrInv);
-    // one barrier per block, set up by its first warp (the driver, with COOP)
-    if (threadIdx.x == 0) mbar_init(s.bar, 1);
+    // one barrier per block, set up by its first warp (the driver, with COOP),
+    // and beside it the wait limit and the record of a wait that ran out
+    if (threadIdx.x == 0) {
+        mbar_init(s.bar, 1);
+        int* const aux = reinterpret_cast<int*>(s.bar + 1);
+        aux[0] = max_polls > 0 ? max_polls : kTmaPolls;
+        aux[1] = 0;
+        aux[2] = 0;
+    }
     fence_proxy_async_smem();
     __syncwarp();
 }
@@ -2073,7 +2112,7 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
     WarpSolver<SIX, Mask, STAGE> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
                  DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
-                 a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy);
+                 a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy, a.tma_max_polls);
     if (DIMC > 0) s.tile_on = a.tile_w > 0;
     s.no_ghost = a.ref_no_ghost != 0;
     const int lane = s.lane, dim = s.dim, half = s.half;
@@ -2151,6 +2190,7 @@ __global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CU
         }
         __syncwarp();
     }
+    s.drain();
 }
 
 // The rescue pass over the tasks the fast pass handed on, with every path of
@@ -2172,7 +2212,7 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
     WarpSolver<SIX, Mask, true, true> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
                  DIMC > 0 ? DIMC : a.dim, a.pitch, L.tile_w, L.tile_h, a.W, a.H, a.min_valid, a.lm, a.ref_pitch,
-                 a.ref_dx, a.ref_dy);
+                 a.ref_dx, a.ref_dy, a.tma_max_polls);
     if (s.warp != 0) {
         s.coop_serve();
         return;
@@ -2245,6 +2285,7 @@ __global__ void __launch_bounds__(kCoopWarps * 32, 1) coop_rescue_kernel(const _
         __syncwarp();
     }
     s.coop_post(0, nullptr);  // done: the other warps leave their loop
+    s.drain();
 }
 
 // The dynamic shared-memory limit of a kernel, always set to the device's

@@ -31,6 +31,7 @@ struct SolveArgs {
     int* deferred;           // n_tasks slots: tasks the fast pass leaves to the general one
     const int* cancel;       // host-mapped cancel flag polled per task, or null
     int* err;                // set to 1 when a TMA wait ran out (the warp then reads global memory)
+    int tma_max_polls;       // polls of a TMA completion wait before it gives up (0: kTmaPolls)
     size_t smem_per_warp;    // set by launch_solve
     int tile_w, tile_h;      // TMA box of the deformed tile, set by launch_solve (0: no tile)
     // set by launch_solve from dim and the shared-memory layout

@@ -10,9 +10,10 @@
 // tasks the fast pass hands on) in a fixed array that is part of the
 // library's device image, so a call allocates nothing.
 //
-// The cost is a fixed 4 MiB array on every GPU that loads the library, held
-// until the process exits, and a limit of DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS
-// tasks per call.
+// The cost is a fixed 4 MiB array on every GPU where the library's device code
+// is loaded (under lazy module loading, from its first use there), held until
+// the process exits, and a limit of DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS tasks per
+// call.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -35,7 +36,9 @@ std::mutex g_mu;
 int* g_scratch[kMaxDevices] = {};
 
 // The scratch's device address on the current device, looked up once per
-// device (with that device current) and cached.
+// device (with that device current) and cached. A reset of the device's
+// primary context reloads the module and moves the array, so the entry is not
+// for use across cudaDeviceReset (the header says so).
 cudaError_t scratch_on_current_device(int** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);

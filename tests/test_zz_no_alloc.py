@@ -13,6 +13,8 @@ The file name sorts last, so a run that stops at the first failure has run
 every other test before this one.
 """
 import ctypes
+import os
+import re
 
 import numpy as np
 import pytest
@@ -23,7 +25,14 @@ pytestmark = pytest.mark.gpu
 
 torch = pytest.importorskip("torch")
 
-MAX_TASKS = 1048576  # DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS in include/semper_dic_cuda.h
+
+def _header_max_tasks():
+    h = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "semper_dic_cuda.h")
+    m = re.search(r"#define\s+DIC_CUDA_SOLVE_NOALLOC_MAX_TASKS\s+(\d+)", open(h).read())
+    return int(m.group(1))
+
+
+MAX_TASKS = _header_max_tasks()  # read from the header the library is built from
 CUDA_ERROR_INVALID_VALUE = 1
 
 
@@ -106,3 +115,20 @@ def test_noalloc_rejects_more_tasks_than_its_scratch_holds():
     rc = _noalloc()(None, None, None, None, 64, 64, 64, None, None, None, 21, 1, 0, None, MAX_TASKS + 1, None, 0,
                     None)
     assert rc == CUDA_ERROR_INVALID_VALUE
+
+
+def test_noalloc_accepts_exactly_the_maximum_task_count():
+    """MAX_TASKS tasks fill the fixed scratch exactly: the call is accepted and
+    solves them as dic_cuda_solve does. The tasks repeat 64 subsets of a small
+    pair (pool rows = task index, tiled on the device)."""
+    args = dict(_cases())["rescue"]
+    n, subset = args[0], args[8]
+    rplanes, dI, (valid, ms, _h, Hs), tasks = _case(*args)
+    reps = MAX_TASKS // len(tasks)
+    assert reps * len(tasks) == MAX_TASKS
+    big = np.tile(tasks, reps)
+    big["node"] = np.arange(MAX_TASKS)
+    pool = (valid.repeat(reps), ms.repeat(reps, 1), None, Hs.repeat(reps, 1))
+    want = sb.solve(rplanes, dI, n, pool, subset, big, lm=True, six=False)
+    got = _run_noalloc(rplanes, dI, n, pool, subset, big, False)
+    assert got.tobytes() == want.tobytes()
