@@ -41,9 +41,27 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
+// Non-blocking probe of the phase with the given parity.
+__device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity to complete: at most
+// max_polls probes, the first one immediate (test_wait), the others allowed
+// to suspend for a while (try_wait). A limit of one poll therefore gives up on
+// any copy not already complete.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int max_polls) {
-    for (int i = 0; i < max_polls; ++i)
+    if (max_polls <= 0) return false;
+    if (mbar_test_wait(bar, parity)) return true;
+    for (int i = 1; i < max_polls; ++i)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
