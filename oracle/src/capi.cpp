@@ -237,7 +237,7 @@ void oracle_ff_inputs(int scenario, uint8_t* ref, uint8_t* def) {
     std::memcpy(def, dd.data(), dd.size());
 }
 
-// ---- incremental session and its per-node math (incremental_core.hpp) ----
+// ---- incremental session and its per-node math (incremental_session.hpp) ----
 
 void* oracle_inc_create() { return new IncSession(); }
 void oracle_inc_destroy(void* p) { delete static_cast<IncSession*>(p); }

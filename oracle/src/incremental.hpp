@@ -1,14 +1,13 @@
 // ORACLE — test infrastructure only. Never linked into the product library.
 //
 // The incremental session over the CPU restatement: the session logic and
-// the per-node math are the shared semper_inc code (incremental_core.hpp),
-// every solve, adoption and packing is the restatement's own (pipeline.hpp,
-// solver.hpp), so a device session and this one agree bit for bit.
+// the per-node math of incremental_session.hpp, every solve, adoption and
+// packing the restatement's own (pipeline.hpp, solver.hpp).
 #pragma once
 
 #include <functional>
 
-#include "../../semper-dic-engine_b200/csrc/host/incremental_core.hpp"
+#include "incremental_session.hpp"
 #include "pipeline.hpp"
 
 namespace oracle {

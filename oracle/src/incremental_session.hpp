@@ -1,11 +1,17 @@
-// Incremental (updated-reference) DIC: the per-node bookkeeping and the
-// session logic, written once for any solver backend.
+// ORACLE — test infrastructure only. Never linked into the product library.
 //
-// Restates src/pipeline/incremental_math.cpp (sampling, coasting fits,
-// anchors, mask warping) and src/pipeline/incremental_session.cpp (the
-// session) of the reference. The device engine (incremental.cpp) and the CPU
-// restatement used by the tests both instantiate IncrementalCore with their
-// own solver, so the two differ only in the solves, which agree bit for bit.
+// Incremental (updated-reference) DIC restated on the CPU: the per-node
+// bookkeeping and the session logic of src/pipeline/incremental_math.cpp
+// (sampling, coasting fits, anchors, mask warping) and
+// src/pipeline/incremental_session.cpp (the session), over the restatement's
+// own solves (incremental.hpp). The device session of the product is a
+// separate implementation; the tests compare the two bit for bit.
+//
+// One definition differs from the reference's text: the length of a coasting
+// step and of a match's shift is the correctly rounded root of the double sum
+// of squares (length2 below), where the reference calls the C library's
+// hypot, whose last bit is the library's own; the device session uses the
+// same definition.
 //
 // The OpenCV operations the reference uses here are restated from their
 // definitions: the exact Euclidean distance transform (distanceTransform,
@@ -25,6 +31,9 @@
 #include <vector>
 
 namespace semper_inc {
+
+// The correctly rounded length of (a, b).
+inline float length2(float a, float b) { return (float)std::sqrt((double)a * a + (double)b * b); }
 
 // include/semper/tuning.hpp:193-281 and the gates the session uses.
 constexpr float kIncTaylorMaxCells = 1.5f;
@@ -433,7 +442,7 @@ inline bool accept_anchor_match(const CoastAnchor& a, int status, float score, f
     if (status != 0 || !(score <= kCorrAccept)) return false;
     const float nx = (float)a.ax + u + (1.0f + ux) * a.dx + uy * a.dy;
     const float ny = (float)a.ay + v + vx * a.dx + (1.0f + vy) * a.dy;
-    if (!(std::hypot(nx - guess_x, ny - guess_y) <= max_shift)) return false;
+    if (!(length2(nx - guess_x, ny - guess_y) <= max_shift)) return false;
     x = nx;
     y = ny;
     corr = score;
@@ -800,7 +809,7 @@ public:
         const int subset_size = params_.subset_size;
         const float max_travel = kIncCoastMaxTravelSubsets * (float)subset_size;
         auto carry = [&](size_t i, float du, float dv) {
-            const float travel = std::hypot(du, dv);
+            const float travel = length2(du, dv);
             if (coast_travel_[i] + travel > max_travel) return;
             U[i] = Ubase_[i] + du;
             V[i] = Vbase_[i] + dv;

@@ -244,6 +244,7 @@ struct Engine::Impl {
     DevBuf<dic::ScatterRec> scat;
     DevBuf<dic::MeshTri> tris;
     DevBuf<uint8_t> valid, fail;
+    DeviceField last_field;  // the field of the last run (device pointers)
     DevBuf<float> exx, eyy, exy;
     DevBuf<unsigned char> pack_scratch;
     DevBuf<float> d_out;
@@ -619,8 +620,8 @@ int Engine::warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, 
     I.mV.ensure(std::max(I.mV.n, ng));
     I.mBox.ensure(4);
     check(cudaMemcpyAsync(I.mMask0.p, mask0, n, cudaMemcpyHostToDevice, st), "H2D material mask");
-    check(cudaMemcpyAsync(I.mU.p, U, ng * 4, cudaMemcpyHostToDevice, st), "H2D U");
-    check(cudaMemcpyAsync(I.mV.p, V, ng * 4, cudaMemcpyHostToDevice, st), "H2D V");
+    check(cudaMemcpyAsync(I.mU.p, U, ng * 4, cudaMemcpyDefault, st), "copy U");
+    check(cudaMemcpyAsync(I.mV.p, V, ng * 4, cudaMemcpyDefault, st), "copy V");
     const dic::MaskField f{gridW, gridH, rect_x, rect_y, step, I.mU.p, I.mV.p};
     I.launched(1, dic::launch_warp_mask(I.mMask0.p, W, H, X0, X1, Y0, Y1, per_px, f, I.mOut.p, st), "mask warp");
     I.launched(2, dic::launch_close3x3(I.mOut.p, I.mTmp.p, W, H, st), "mask close");
@@ -641,6 +642,8 @@ int Engine::warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, 
 }
 int vsg_window_nodes(int step, int window) { return vsg_window_node_count(step, window); }
 
+DeviceField Engine::last_field() const { return impl_->last_field; }
+
 int Engine::pack_field(int gW, int gH, int rect_x, int rect_y, int step, int window, const float* u, const float* v,
                        const float* corr, const uint8_t* solved, float* out, int capacity) {
     Impl& I = *impl_;
@@ -649,10 +652,12 @@ int Engine::pack_field(int gW, int gH, int rect_x, int rect_y, int step, int win
     for (DevBuf<float>* b : {&I.fu, &I.fv, &I.fux, &I.fuy, &I.fvx, &I.fvy, &I.fcorr}) b->ensure(std::max(b->n, NG));
     I.fsolved.ensure(std::max(I.fsolved.n, NG));
     I.fiters.ensure(std::max(I.fiters.n, NG));
-    check(cudaMemcpyAsync(I.fu.p, u, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D u");
-    check(cudaMemcpyAsync(I.fv.p, v, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D v");
-    check(cudaMemcpyAsync(I.fcorr.p, corr, NG * 4, cudaMemcpyHostToDevice, stream_), "H2D corr");
-    check(cudaMemcpyAsync(I.fsolved.p, solved, NG, cudaMemcpyHostToDevice, stream_), "H2D solved");
+    // host or device inputs (unified addressing tells them apart)
+    check(cudaMemcpyAsync(I.fu.p, u, NG * 4, cudaMemcpyDefault, stream_), "copy u");
+    check(cudaMemcpyAsync(I.fv.p, v, NG * 4, cudaMemcpyDefault, stream_), "copy v");
+    check(cudaMemcpyAsync(I.fcorr.p, corr, NG * 4, cudaMemcpyDefault, stream_), "copy corr");
+    check(cudaMemcpyAsync(I.fsolved.p, solved, NG, cudaMemcpyDefault, stream_), "copy solved");
+    I.last_field = DeviceField{};
     const int cap = std::max(capacity, 0);
     I.d_out.ensure(std::max<size_t>(I.d_out.n, (size_t)std::max(cap, 8)));
     int dropped_outlier = 0, dropped_post = 0;
@@ -751,6 +756,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
     E.times_ = PhaseTimes{};
     E.last_global_ = dic::GlobalSimilarity();
     last_def = d_def;
+    last_field = DeviceField{};
     try {
         poll_cancel();
         check(cudaEventRecord(ev[0], st), "event");
@@ -1417,6 +1423,8 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         int dropped_outlier = 0, dropped_post = 0;
         const int valid_count = strain_pack(gW, gH, params.rect_x, params.rect_y, params.step, params.strain_window,
                                             d_out_p, capacity, dropped_outlier, dropped_post);
+        last_field = DeviceField{gW, gH, params.rect_x, params.rect_y, params.step, total, fu.p, fv.p, fux.p, fuy.p,
+                                 fvx.p, fvy.p, fcorr.p, fsolved.p, valid.p};
         if (capture) {
             capture->median_valid.resize(NG);
             check(cudaMemcpyAsync(capture->median_valid.data(), valid.p, NG, cudaMemcpyDeviceToHost, st),

@@ -76,6 +76,17 @@ struct Capture {
     int median_rejected = 0;
 };
 
+// The per-node state of the last solve, left in device memory (the same
+// nodes as Capture): valid until the next call on the engine that solves or
+// packs. `ok` holds the packing's displacement median flags.
+struct DeviceField {
+    int gridW = 0, gridH = 0, rect_x = 0, rect_y = 0, step = 0, attempted = 0;
+    const float *u = nullptr, *v = nullptr, *ux = nullptr, *uy = nullptr, *vx = nullptr, *vy = nullptr,
+                *corr = nullptr;
+    const uint8_t* solved = nullptr;
+    const uint8_t* ok = nullptr;
+};
+
 // Timings of one solve's device phases, measured with CUDA events on the
 // engine's stream (ms).
 struct PhaseTimes {
@@ -130,9 +141,13 @@ public:
                    float* metrics, int metrics_len, const double* model_H = nullptr, Progress progress = nullptr,
                    Capture* capture = nullptr);
 
-    // pack_full_field_output over a host grid (gW x gH nodes at rect + i *
-    // step): the displacement median test, VSG strain and packing on the
-    // device, out (host) receiving the points. Returns the points written.
+    // The field of the last run, in device memory.
+    DeviceField last_field() const;
+
+    // pack_full_field_output over a grid (gW x gH nodes at rect + i * step;
+    // u, v, corr, solved in host or device memory): the displacement median
+    // test, VSG strain and packing on the device, out (host) receiving the
+    // points. Returns the points written.
     int pack_field(int gW, int gH, int rect_x, int rect_y, int step, int window, const float* u, const float* v,
                    const float* corr, const uint8_t* solved, float* out, int capacity);
 
@@ -143,7 +158,7 @@ public:
     PatchSolve solve_patch(const uint8_t* patch, int size, int ax, int ay, float gu, float gv, int subset, bool six);
 
     // warp_material_mask's scatter and close (incremental_math.cpp:371-447)
-    // on the device: every material pixel (mask0 >= 128) of the window
+    // on the device (U, V in host or device memory): every material pixel (mask0 >= 128) of the window
     // [X0, X1] x [Y0, Y1] sends per_px x per_px samples X to X + U(X), U the
     // filled field of the grid; then a 3x3 close. out (host, W x H) receives
     // the mask; box = {x, y, w, h} of its nonzero pixels (all 0 if none).

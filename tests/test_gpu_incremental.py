@@ -2,9 +2,11 @@
 restatement (include/semper/incremental.hpp; tests/integration/
 test_incremental.cpp of the reference for the contracts checked here).
 
-Both sessions run the shared session logic; their solves, reference
-adoptions and packing agree bit for bit, so every frame's points, return
-code and frame info must be identical.
+The device session (per-node state and steps as kernels, incnode.cu and
+inc_session.cpp) and the CPU restatement's session
+(oracle/src/incremental_session.hpp) are separate implementations of the
+same rules; their solves, reference adoptions and packing agree bit for bit,
+so every frame's points, return code and frame info must be identical.
 """
 import numpy as np
 import pytest
@@ -125,3 +127,39 @@ def test_cancel_during_frame():
     rb, pb, _, ib = b.process(j["dfm"], cap)
     assert ra == rb > 0 and np.array_equal(pa, pb)
     assert ia.reference_frame == ib.reference_frame
+
+
+def strip_sequence(n=320, frames=12, seed=41, speed=1.6, x0=150, width=14):
+    """Material translating and stretching under a stationary, textureless
+    band: subsets that overlap the band cannot be matched, so their nodes
+    coast on fitted planes while the band covers them and, once past it, are
+    confirmed only by direct matches of their anchors (cut where they were
+    last clean)."""
+    ref = sb.speckle(n, n, seed)
+    out = []
+    for t in range(1, frames + 1):
+        w = sb.warp_block(cx=n / 2, cy=n / 2, u0=speed * t, v0=-0.3 * t, a=(0.002 * t, 0.0, 0.0, -0.001 * t))
+        f = sb.speckle(n, n, seed, w, 1.0, 300 + t)
+        f[:, x0:x0 + width] = 128
+        out.append(f)
+    return ref, out
+
+
+@pytest.mark.parametrize("interval", [1, 2])
+def test_coasting_and_anchor_matches_match_restatement(interval):
+    ref, frames = strip_sequence()
+    dev = sb.Incremental()
+    ora = oracle.IncrementalOracle()
+    assert dev.init(ref, sb.params((16, 16, 288, 288), 8, 21, 21), interval) == 0
+    assert ora.init(ref, [16, 16, 288, 288, 8, 21, 21, 0], interval) == 0
+    cap = 36 * 36 * 8
+    matches = taylor = 0
+    for f in frames:
+        d = dev.process(f, cap)
+        o = ora.process(f, cap)
+        assert_same(d, o)
+        matches += int(dev.profile()["matches"])
+        taylor += d[3].taylor_fallbacks
+    print(f"interval {interval}: {matches} anchor matches, {taylor} Taylor samples")
+    assert taylor > 0
+    assert matches > 0

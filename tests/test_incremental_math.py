@@ -2,8 +2,9 @@
 fit, anchors, the node field of a solve and the material-mask warp.
 
 Known answers of the reference's tests/unit/test_incremental_math.cpp, run on
-the shared restatement (semper-dic-engine_b200/csrc/host/incremental_core.hpp)
-through the oracle library: the device session uses the same code.
+the CPU restatement (oracle/src/incremental_session.hpp) through the oracle
+library. The device session (incnode.cu) is a separate implementation, held
+to this restatement bit for bit by the GPU incremental tests.
 """
 import math
 
