@@ -3,6 +3,7 @@
 // engine — per-handle busy guard, per-handle cancel token with the reference's
 // cancel window (include/semper/cancel.hpp:53-110), and an exception barrier
 // at every entry (include/semper/guarded_call.hpp:22-44).
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstdint>
@@ -14,6 +15,7 @@
 #include "../../../include/semper_b200_ext.h"
 #include "../../../include/semper_c.h"
 #include "engine.hpp"
+#include "gray.hpp"
 #include "incremental.hpp"
 
 using semper_b200::Engine;
@@ -63,8 +65,10 @@ Params to_params(const semper_params* p) {
 }
 
 // io::decode_gray for raw buffers (src/io/image_codec.cpp:126-160): ALPHA_8
-// when len == w*h, RGBA when len == 4*w*h (BT.601 luma, rounded). Encoded
-// images are not decoded by this build: empty result.
+// when len == w*h, RGBA when len == 4*w*h (cvtColor RGBA2GRAY's fixed-point
+// BT.601 luma, gray.hpp). Encoded images are not decoded by this build: empty
+// result (a raw buffer is taken as raw even when its first bytes look like an
+// image file's signature).
 bool decode_raw(const uint8_t* data, size_t len, int w, int h, std::vector<uint8_t>& out) {
     if (!data || len == 0 || w <= 0 || h <= 0) return false;
     const uint64_t px = (uint64_t)w * (uint64_t)h;
@@ -75,11 +79,7 @@ bool decode_raw(const uint8_t* data, size_t len, int w, int h, std::vector<uint8
     }
     if ((uint64_t)len == 4 * px) {
         out.resize(px);
-        for (uint64_t i = 0; i < px; ++i) {
-            const double y = 0.299 * data[4 * i] + 0.587 * data[4 * i + 1] + 0.114 * data[4 * i + 2];
-            const long r = std::lround(y);
-            out[i] = (uint8_t)(r < 0 ? 0 : (r > 255 ? 255 : r));
-        }
+        semper_b200::rgba_to_gray(data, (size_t)px, out.data());
         return true;
     }
     return false;

@@ -1,4 +1,4 @@
-"""Python binding of libsemper_c.so (ctypes) and of the speckle generator.
+"""Python binding of libsemper_b200.so (ctypes) and of the speckle generator.
 
 The engine is the C ABI of include/semper_c.h; the stage entries are the
 kernel-level C ABI of include/semper_dic_cuda.h, here driven with torch device
@@ -15,7 +15,10 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libsemper_c.so")
+# The full library (C ABI, extensions, stage ABI, C++ API). libsemper_c.so is
+# the same code exporting only the reference's eleven C-ABI symbols.
+LIB_PATH = os.path.join(HERE, "lib", "libsemper_b200.so")
+C_LIB_PATH = os.path.join(HERE, "lib", "libsemper_c.so")
 SYNTH_PATH = os.path.join(HERE, "lib", "libsemper_synth.so")
 
 _u8p = ctypes.POINTER(ctypes.c_uint8)
@@ -188,6 +191,12 @@ class Engine:
         m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
         return lib().semper_set_reference(self._h, _p(g, _u8p), g.size, _p(m, _u8p), 0 if m is None else m.size,
                                           g.shape[1], g.shape[0])
+
+    def set_reference_bytes(self, data: bytes, width: int, height: int) -> int:
+        """semper_set_reference with a raw buffer as the reference's decoding
+        takes it (width*height gray bytes, or 4*width*height RGBA)."""
+        buf = np.frombuffer(data, np.uint8)
+        return lib().semper_set_reference(self._h, _p(buf, _u8p), buf.size, None, 0, width, height)
 
     def run(self, deformed: np.ndarray, prm: SemperParams, capacity: int | None = None, mask=None,
             metrics_len: int = 24, progress=None, out: np.ndarray | None = None):
