@@ -445,7 +445,7 @@ def run_cfg3(args, rank):
     cap = ((n - 2 * m) // 6) ** 2 * 8
     inc = sb.Incremental()
     assert inc.init(ref, prm, args.interval) == 0
-    ms, pts, updates = [], [], 0
+    ms, pts, updates, profs = [], [], 0, []
     with ClockSampler(0) as clk:
         for i, f in enumerate(frames):
             torch.cuda.synchronize()
@@ -457,6 +457,7 @@ def run_cfg3(args, rank):
                 ms.append(1000 * dt)
                 pts.append(rc)
                 updates += info.reference_updated
+                profs.append(inc.profile())
     mean_ms = statistics.mean(ms)
     line = {
         "metric": METRIC, "value": sum(pts) / (sum(ms) / 1000.0), "unit": "points/s", "n_gpus": 1,
@@ -467,6 +468,8 @@ def run_cfg3(args, rank):
                                f"frames {args.warmup + 1}..{total} timed after {args.warmup} warm-up frames",
                    "frames_timed": len(ms), "reference_updates": updates, "points_per_frame": statistics.mean(pts)},
         "frames_per_s": 1000.0 / mean_ms,
+        "frame_profile_ms": {k: round(statistics.mean(p[k] for p in profs), 3)
+                             for k in ("total", "run", "match", "warp_mask", "adopt", "pack", "matches")},
         "e2e": {"value": sum(pts) / (sum(ms) / 1000.0), "unit": "points/s", "h2d_bytes_per_step": n * n,
                 "d2h_bytes_per_step": int(statistics.mean(pts)) * 32},
         "clocks": clk.summary(),

@@ -116,6 +116,54 @@ SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jo
    none; valid until the next call on the runner. */
 SEMPER_C_API const char* semper_b200_batch_last_error(semper_b200_batch* b);
 
+/* The learned seed proposal network (no counterpart in the reference): two
+   64x64 patches in, the 6-parameter affine map between them out; BF16
+   tensor-core kernels with FP32 accumulation for inference and training.
+   Parameters are `semper_b200_proposal_param_count()` floats in the layout
+   w0 b0 ... w4 b4 (convolutions [co][kh][kw][ci]) w5 b5 w6 b6 (dense
+   [out][in]). Patches are [batch][64][64][2] floats (NHWC), outputs
+   [batch][6]: A = I + [[o0, o1], [o2, o3]], t = 16 (o4, o5) in patch
+   pixels. Every call returns 0, or -3 for a NULL handle or a bad argument. */
+typedef struct semper_b200_proposal semper_b200_proposal;
+SEMPER_C_API semper_b200_proposal* semper_b200_proposal_create(int32_t max_batch);
+SEMPER_C_API void semper_b200_proposal_destroy(semper_b200_proposal* p);
+SEMPER_C_API int64_t semper_b200_proposal_param_count(void);
+SEMPER_C_API int semper_b200_proposal_set_params(semper_b200_proposal* p, const float* params, int64_t n);
+SEMPER_C_API int semper_b200_proposal_get_params(semper_b200_proposal* p, float* params, int64_t n);
+/* Forward over a batch of patch pairs (host memory). */
+SEMPER_C_API int semper_b200_proposal_forward(semper_b200_proposal* p, const float* x, int32_t batch, float* out);
+/* The loss of `target` [batch][6] (the mean squared displacement error of the
+   affine map at a 3x3 grid of patch points, patch px^2) and the gradient of
+   every parameter. */
+SEMPER_C_API int semper_b200_proposal_gradients(semper_b200_proposal* p, const float* x, const float* target,
+                                                int32_t batch, float* grads, float* loss);
+/* Synthetic pairs from a w x h u8 speckle image: cfg = {max rotation (rad),
+   max stretch, max shear, max shift (px), noise (gray levels), box factor}. */
+SEMPER_C_API int semper_b200_proposal_synth(semper_b200_proposal* p, const uint8_t* speckle, int32_t w, int32_t h,
+                                            const float cfg[6], uint64_t seed, int32_t batch, float* x,
+                                            float* target);
+/* `steps` Adam steps on batches of synthetic pairs; losses[steps] (may be
+   NULL) receives each batch's loss. */
+SEMPER_C_API int semper_b200_proposal_train(semper_b200_proposal* p, const uint8_t* speckle, int32_t w, int32_t h,
+                                            const float cfg[6], int32_t steps, int32_t batch, float lr,
+                                            uint64_t seed, float* losses);
+
+/* Learned seeding on an engine handle: with a proposal network (NULL: none)
+   and learned != 0, a run with no model set proposes its global model from
+   the network's predictions on patch pairs of the reference and the
+   deformed frame; the anchor lattice keeps or rejects it by the reference's
+   keep rule (full_field_anchors.cpp:204-279), and a rejected proposal falls
+   back to the global-motion estimate. The network must stay alive while the
+   handle may use it. Returns 0, or -3 for a NULL or busy handle. */
+SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_proposal* p, int learned);
+
+/* The last run's learned seeding: out[0] 1 when it ran, [1] a model was
+   proposed, [2] the lattice kept it; [3] patch pairs, [4] inlier pairs of the
+   fit, [5] anchors that judged it, [6] their mean and [7] largest distance
+   from the proposal (px), [8] device time of the network's stages (ms),
+   [9..17] the proposed homography (row-major). Returns 0, or -3. */
+SEMPER_C_API int semper_b200_last_learned(semper_engine* eng, double out[18]);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -14,6 +14,7 @@
 //   median test, VSG, packing (full_field_solver_stats.cpp:21-91)           strain kernels
 //   metrics (full_field_solver_stats.cpp:182-280)                           host
 #include "engine.hpp"
+#include "proposal.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -360,6 +361,95 @@ struct Engine::Impl {
         if (t.best >= 0 || !(ms_per_pixel_iter > 0.0)) return;
         if (t.t[variant] == 0.0 || ms_per_pixel_iter < t.t[variant]) t.t[variant] = ms_per_pixel_iter;
         if (++t.trials >= kTuneTrials) t.best = t.t[1] < t.t[0] ? 1 : 0;
+    }
+
+    // The learned proposal of the global model: the network's predictions on
+    // patch pairs (box factor 4, 256 px a side), first five pairs at the ROI
+    // centre (the same place in both frames) whose median affine map places
+    // a 6 x 6 grid of pairs over the central 70 % of the ROI, then a
+    // homography fitted to where that grid's patch origins land (DLT with an
+    // inlier refit at 6 px). False when the fit fails.
+    bool learned_model(const Params& params, const uint8_t* d_def, double H[9]) {
+        LearnedSeed& L = E.last_learned_;
+        L = LearnedSeed{};
+        L.ran = true;
+        ProposalNet& net = *E.proposal_;
+        cudaStream_t st = E.stream_;
+        const int W = E.W_, Hh = E.H_, f = 4;
+        cudaEvent_t e0, e1;
+        check(cudaEventCreate(&e0), "event");
+        check(cudaEventCreate(&e1), "event");
+        check(cudaEventRecord(e0, st), "event");
+        const int cx = params.rect_x + params.rect_w / 2, cy = params.rect_y + params.rect_h / 2;
+        const int off[5][2] = {{0, 0}, {24, 0}, {-24, 0}, {0, 24}, {0, -24}};
+        float c1[5 * 4], o1[5 * 6];
+        for (int k = 0; k < 5; ++k) {
+            c1[4 * k] = c1[4 * k + 2] = (float)(cx + off[k][0]);
+            c1[4 * k + 1] = c1[4 * k + 3] = (float)(cy + off[k][1]);
+        }
+        net.predict_device(rGray.p, d_def, W, Hh, W, c1, 5, f, o1, st);
+        // x' = A x + b per pair, about its origin c - 0.5; the median entry-wise
+        std::vector<double> comp[6];
+        for (int k = 0; k < 5; ++k) {
+            const double a00 = 1.0 + o1[6 * k], a01 = o1[6 * k + 1], a10 = o1[6 * k + 2], a11 = 1.0 + o1[6 * k + 3];
+            const double tx = f * dic::kPpTScale * o1[6 * k + 4], ty = f * dic::kPpTScale * o1[6 * k + 5];
+            const double ox = c1[4 * k] - 0.5, oy = c1[4 * k + 1] - 0.5;
+            comp[0].push_back(a00);
+            comp[1].push_back(a01);
+            comp[2].push_back(a10);
+            comp[3].push_back(a11);
+            comp[4].push_back(ox + tx - (a00 * ox + a01 * oy));
+            comp[5].push_back(oy + ty - (a10 * ox + a11 * oy));
+        }
+        double m[6];
+        for (int i = 0; i < 6; ++i) {
+            std::sort(comp[i].begin(), comp[i].end());
+            m[i] = comp[i][2];
+        }
+        // the grid of pairs, each placed by the centre's map
+        constexpr int G = 6;
+        std::vector<float> c2;
+        std::vector<semper_geom::Pt> rp, dp;
+        for (int j = 0; j < G; ++j)
+            for (int i = 0; i < G; ++i) {
+                const int rx = params.rect_x + (int)(params.rect_w * (0.15 + 0.7 * (i + 0.5) / G));
+                const int ry = params.rect_y + (int)(params.rect_h * (0.15 + 0.7 * (j + 0.5) / G));
+                const double X = rx - 0.5, Y = ry - 0.5;
+                const double px = m[0] * X + m[1] * Y + m[4] + 0.5, py = m[2] * X + m[3] * Y + m[5] + 0.5;
+                if (!(px > 0.0 && py > 0.0 && px < W - 1 && py < Hh - 1)) continue;
+                c2.insert(c2.end(), {(float)rx, (float)ry, (float)std::lround(px), (float)std::lround(py)});
+            }
+        const int K = (int)c2.size() / 4;
+        L.pairs = K;
+        bool ok = false;
+        if (K >= 8 && K <= net.max_batch()) {
+            std::vector<float> o2((size_t)K * 6);
+            net.predict_device(rGray.p, d_def, W, Hh, W, c2.data(), K, f, o2.data(), st);
+            for (int k = 0; k < K; ++k) {
+                rp.push_back({c2[4 * k] - 0.5, c2[4 * k + 1] - 0.5});
+                dp.push_back({c2[4 * k + 2] - 0.5 + f * dic::kPpTScale * o2[6 * k + 4],
+                              c2[4 * k + 3] - 0.5 + f * dic::kPpTScale * o2[6 * k + 5]});
+            }
+            ok = semper_geom::fit_homography(rp, dp, 6.0, H);
+            if (ok) {
+                for (int k = 0; k < K; ++k) {
+                    double X, Y, J[4];
+                    if (semper_geom::homography_at(H, rp[k].x, rp[k].y, X, Y, J) &&
+                        std::hypot(X - dp[k].x, Y - dp[k].y) <= 6.0)
+                        L.inliers++;
+                }
+                ok = L.inliers >= 8;
+            }
+        }
+        check(cudaEventRecord(e1, st), "event");
+        check(cudaEventSynchronize(e1), "event");
+        cudaEventElapsedTime(&L.ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        E.times_.launches += 2 * 14;
+        L.proposed = ok;
+        if (ok) std::copy(H, H + 9, L.H);
+        return ok;
     }
 
     dic::SolveArgs solve_args(int dim, int six) {
@@ -830,18 +920,27 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
 
         // ---------------------------------------------------------------- global model
         const auto t_seed = clk::now();
-        if (!model_H && E.global_motion_ && ref_gray) {
-            dic::GlobalSimilarity& g = E.last_global_;
-            check(gm.estimate(rGray.p, d_def, W, H, params.rect_x, params.rect_y, params.rect_w, params.rect_h, st, g),
-                  "global motion");
-            E.times_.launches += g.kernels;
-            if (g.locked) model_H = g.H;
-        }
+        E.last_learned_ = LearnedSeed{};
+        double learned_H[9];
+        const bool learned = !model_H && ref_gray && E.learned_ && E.proposal_ &&
+                             learned_model(params, d_def, learned_H);
+        if (learned) model_H = learned_H;
+        auto plain_estimate = [&]() {
+            if (!model_H && E.global_motion_ && ref_gray) {
+                dic::GlobalSimilarity& g = E.last_global_;
+                check(gm.estimate(rGray.p, d_def, W, H, params.rect_x, params.rect_y, params.rect_w, params.rect_h,
+                                  st, g),
+                      "global motion");
+                E.times_.launches += g.kernels;
+                if (g.locked) model_H = g.H;
+            }
+        };
+        plain_estimate();
 
         // ---------------------------------------------------------------- anchor lattice
         HostStats st_anchor, st_a, st_b;
         float globalU = 0, globalV = 0;
-        bool have_model = model_H != nullptr, model_full = false, model_rejected = false;
+        bool have_model = false, model_full = false, model_rejected = false;
         double t_u = 0, t_v = 0;
         Quality quality = Quality::NONE;
         float coverage = 0.f;
@@ -856,6 +955,13 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             g6[4] = (float)J[2]; g6[5] = (float)(J[3] - 1.0);
             return true;
         };
+        bool locked = false;
+        std::vector<double> homography;
+        // The model's guesses and its reach over the ROI (full_field_anchors.cpp:204-279).
+        auto setup_model = [&]() {
+        have_model = model_H != nullptr;
+        model_full = model_rejected = false;
+        t_u = t_v = 0;
         if (have_model) {
             const double gcx = params.rect_x + 0.5 * params.rect_w, gcy = params.rect_y + 0.5 * params.rect_h;
             float g6[6];
@@ -872,9 +978,11 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                             model_full = true;
             }
         }
-        const bool locked = have_model;
-        std::vector<double> homography;
+        locked = have_model;
+        homography.clear();
         if (have_model) homography.assign(model_H, model_H + 9);
+        };
+        setup_model();
 
         int sx, sy;
         plan_lattice(gW, gH, sx, sy);
@@ -989,6 +1097,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             return frac;
         };
 
+        auto seed_lattice = [&]() {
         if (LW >= 2 && LH >= 2) {
             if (!model_full) {
                 solve_lattice(false);
@@ -1011,6 +1120,34 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         } else {
             globalU = (float)t_u;
             globalV = (float)t_v;
+        }
+        };
+        seed_lattice();
+        if (learned) {
+            // the lattice judges the proposal: its error against the anchors
+            // solved under it, and whether the keep rule held
+            LearnedSeed& Ls = E.last_learned_;
+            double se = 0.0;
+            for (const Anchor& a : anchors) {
+                if (!a.vertex) continue;
+                float g6[6];
+                if (!model_at(a.rx, a.ry, g6)) continue;
+                const float e = std::hypot(a.u - g6[0], a.v - g6[1]);
+                se += e;
+                Ls.err_max = std::max(Ls.err_max, e);
+                Ls.anchors++;
+            }
+            Ls.err_mean = Ls.anchors ? (float)(se / Ls.anchors) : 0.f;
+            Ls.kept = have_model && !model_rejected;
+            if (!Ls.kept) {
+                // rejected: seed again from the global-motion estimate, the
+                // anchors' statistics counted for that seeding only
+                st_anchor = HostStats();
+                model_H = nullptr;
+                plain_estimate();
+                setup_model();
+                seed_lattice();
+            }
         }
         // publish_anchor_results (full_field_anchors.cpp:576-607)
         {

@@ -104,6 +104,21 @@ int check_params(Params& p, int width, int height);
 // StrainCalculator::vsg_window_node_count (strain_calculator.cpp:12-25).
 int vsg_window_nodes(int step, int window);
 
+class ProposalNet;
+
+// What the learned seeding did in the last run: whether it ran, the model it
+// proposed (reference -> deformed homography, fitted to the network's patch
+// predictions), whether the anchor lattice kept that model (else the
+// global-motion estimate took over), and the proposal's error against the
+// lattice's own IC-GN solutions (px, over the anchors solved under it).
+struct LearnedSeed {
+    bool ran = false, proposed = false, kept = false;
+    double H[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    int pairs = 0, inliers = 0, anchors = 0;
+    float err_mean = 0.0f, err_max = 0.0f;
+    float ms = 0.0f;  // device time of the network's stages
+};
+
 // The raw result of one patch-subset solve (match_anchor's solve).
 struct PatchSolve {
     bool initialized = false;
@@ -180,6 +195,17 @@ public:
     // The estimate of the last run (locked false: none, or none used).
     const dic::GlobalSimilarity& last_global() const { return last_global_; }
 
+    // Learned seeding: with a proposal network set (not owned) and `learned`
+    // on, a run with no model given proposes its global model from the
+    // network's predictions on patch pairs of the reference and the deformed
+    // frame; the anchor lattice judges it by the reference's keep rule and,
+    // if it is rejected, the run seeds again from the global-motion estimate.
+    void set_proposal(ProposalNet* net, bool learned) {
+        proposal_ = net;
+        learned_ = learned && net != nullptr;
+    }
+    const LearnedSeed& last_learned() const { return last_learned_; }
+
     cudaStream_t stream() const { return stream_; }
     const PhaseTimes& last_times() const { return times_; }
     // The fast pass's shape the autotuner kept for (subset size, interpolator):
@@ -209,6 +235,9 @@ private:
     int last_tma_timeout_ = 0;
     bool global_motion_ = true;
     dic::GlobalSimilarity last_global_;
+    ProposalNet* proposal_ = nullptr;
+    bool learned_ = false;
+    LearnedSeed last_learned_;
     PhaseTimes times_;
     friend struct Impl;
 };

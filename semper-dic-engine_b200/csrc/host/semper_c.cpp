@@ -17,6 +17,7 @@
 #include "engine.hpp"
 #include "gray.hpp"
 #include "incremental.hpp"
+#include "proposal.hpp"
 
 using semper_b200::Engine;
 using semper_b200::IncrementalSession;
@@ -359,6 +360,128 @@ SEMPER_C_API int semper_incremental_process(semper_incremental* inc, const uint8
 
 SEMPER_C_API void semper_incremental_cancel(semper_incremental* inc) {
     if (inc != nullptr && inc->session) inc->session->engine().request_cancel();
+}
+
+}  // extern "C"
+
+struct semper_b200_proposal {
+    std::unique_ptr<semper_b200::ProposalNet> net;
+};
+
+namespace {
+
+dic::PpSynth synth_cfg(const float cfg[6]) {
+    dic::PpSynth c;
+    c.max_rot = cfg[0];
+    c.max_stretch = cfg[1];
+    c.max_shear = cfg[2];
+    c.max_shift = cfg[3];
+    c.noise = cfg[4];
+    c.f = (int)cfg[5];
+    return c;
+}
+
+// Synthetic pairs must fit the speckle image with their whole warped reach.
+bool synth_ok(const uint8_t* speckle, int32_t w, int32_t h, const float* cfg) {
+    if (!speckle || !cfg || w < 64 || h < 64) return false;
+    const int f = (int)cfg[5];
+    if (f < 1 || f > 16 || !(cfg[1] >= 0.0f && cfg[1] < 0.5f) || !(cfg[2] >= 0.0f && cfg[2] < 0.5f) ||
+        !(cfg[3] >= 0.0f) || !(cfg[4] >= 0.0f))
+        return false;
+    const float reach = 32.0f * f * 1.4143f * (1.0f + cfg[1] + cfg[2]) + cfg[3] + 4.0f;
+    return 2.0f * reach < (float)std::min(w, h);
+}
+
+}  // namespace
+
+extern "C" {
+
+SEMPER_C_API semper_b200_proposal* semper_b200_proposal_create(int32_t max_batch) {
+    return guarded<semper_b200_proposal*>(nullptr, [&] {
+        auto* p = new semper_b200_proposal();
+        p->net.reset(new semper_b200::ProposalNet(max_batch));
+        return p;
+    });
+}
+
+SEMPER_C_API void semper_b200_proposal_destroy(semper_b200_proposal* p) { delete p; }
+
+SEMPER_C_API int64_t semper_b200_proposal_param_count(void) {
+    return (int64_t)semper_b200::ProposalNet::param_count();
+}
+
+SEMPER_C_API int semper_b200_proposal_set_params(semper_b200_proposal* p, const float* params, int64_t n) {
+    if (!p || !params || n != (int64_t)semper_b200::ProposalNet::param_count()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->set_params(params);
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_proposal_get_params(semper_b200_proposal* p, float* params, int64_t n) {
+    if (!p || !params || n != (int64_t)semper_b200::ProposalNet::param_count()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->get_params(params);
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_proposal_forward(semper_b200_proposal* p, const float* x, int32_t batch, float* out) {
+    if (!p || !x || !out || batch <= 0 || batch > p->net->max_batch()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->forward_host(x, batch, out);
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_proposal_gradients(semper_b200_proposal* p, const float* x, const float* target,
+                                                int32_t batch, float* grads, float* loss) {
+    if (!p || !x || !target || !grads || batch <= 0 || batch > p->net->max_batch()) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        const float l = p->net->gradients_host(x, target, batch, grads);
+        if (loss) *loss = l;
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_proposal_synth(semper_b200_proposal* p, const uint8_t* speckle, int32_t w, int32_t h,
+                                            const float cfg[6], uint64_t seed, int32_t batch, float* x,
+                                            float* target) {
+    if (!p || !x || !target || batch <= 0 || batch > p->net->max_batch() || !synth_ok(speckle, w, h, cfg))
+        return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->synth_host(speckle, w, h, synth_cfg(cfg), seed, batch, x, target);
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_proposal_train(semper_b200_proposal* p, const uint8_t* speckle, int32_t w, int32_t h,
+                                            const float cfg[6], int32_t steps, int32_t batch, float lr,
+                                            uint64_t seed, float* losses) {
+    if (!p || steps < 0 || batch <= 0 || batch > p->net->max_batch() || !synth_ok(speckle, w, h, cfg))
+        return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->train(speckle, w, h, synth_cfg(cfg), steps, batch, lr, seed, losses);
+        return 0;
+    });
+}
+
+SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_proposal* p, int learned) {
+    if (eng == nullptr) return SEMPER_ERR_INIT;
+    HandleCall call(eng->busy);
+    if (!call.owned()) return SEMPER_ERR_INIT;
+    eng->engine.set_proposal(p ? p->net.get() : nullptr, learned != 0);
+    return 0;
+}
+
+SEMPER_C_API int semper_b200_last_learned(semper_engine* eng, double out[18]) {
+    if (eng == nullptr || out == nullptr) return SEMPER_ERR_INIT;
+    const semper_b200::LearnedSeed& L = eng->engine.last_learned();
+    const double v[9] = {L.ran ? 1.0 : 0.0, L.proposed ? 1.0 : 0.0, L.kept ? 1.0 : 0.0, (double)L.pairs,
+                         (double)L.inliers, (double)L.anchors, L.err_mean, L.err_max, L.ms};
+    for (int i = 0; i < 9; ++i) out[i] = v[i];
+    for (int i = 0; i < 9; ++i) out[9 + i] = L.H[i];
+    return 0;
 }
 
 }  // extern "C"

@@ -42,7 +42,11 @@ EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b20
                "semper_b200_stream", "semper_b200_set_global_motion", "semper_b200_last_global_motion",
                "semper_b200_batch_create", "semper_b200_batch_destroy", "semper_b200_batch_run",
                "semper_b200_batch_last_error", "semper_b200_incremental_profile", "semper_b200_fast_pass_shape",
-               "semper_b200_set_tma_wait_limit", "semper_b200_last_tma_timeout"]
+               "semper_b200_set_tma_wait_limit", "semper_b200_last_tma_timeout",
+               "semper_b200_proposal_create", "semper_b200_proposal_destroy", "semper_b200_proposal_param_count",
+               "semper_b200_proposal_set_params", "semper_b200_proposal_get_params", "semper_b200_proposal_forward",
+               "semper_b200_proposal_gradients", "semper_b200_proposal_synth", "semper_b200_proposal_train",
+               "semper_b200_set_proposal", "semper_b200_last_learned"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -110,6 +114,20 @@ def lib():
         L.semper_b200_set_global_model.argtypes = [_vp, _f64p]
         L.semper_b200_fast_pass_shape.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
         L.semper_b200_set_global_motion.argtypes = [_vp, ctypes.c_int]
+        L.semper_b200_proposal_create.argtypes = [ctypes.c_int32]
+        L.semper_b200_proposal_create.restype = _vp
+        L.semper_b200_proposal_destroy.argtypes = [_vp]
+        L.semper_b200_proposal_param_count.restype = ctypes.c_int64
+        L.semper_b200_proposal_set_params.argtypes = [_vp, _f32p, ctypes.c_int64]
+        L.semper_b200_proposal_get_params.argtypes = [_vp, _f32p, ctypes.c_int64]
+        L.semper_b200_proposal_forward.argtypes = [_vp, _f32p, ctypes.c_int32, _f32p]
+        L.semper_b200_proposal_gradients.argtypes = [_vp, _f32p, _f32p, ctypes.c_int32, _f32p, _f32p]
+        L.semper_b200_proposal_synth.argtypes = [_vp, _u8p, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_uint64,
+                                                 ctypes.c_int32, _f32p, _f32p]
+        L.semper_b200_proposal_train.argtypes = [_vp, _u8p, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_int32,
+                                                 ctypes.c_int32, ctypes.c_float, ctypes.c_uint64, _f32p]
+        L.semper_b200_set_proposal.argtypes = [_vp, _vp, ctypes.c_int]
+        L.semper_b200_last_learned.argtypes = [_vp, _f64p]
         L.semper_b200_set_tma_wait_limit.argtypes = [_vp, ctypes.c_int]
         L.semper_b200_last_tma_timeout.argtypes = [_vp]
         L.semper_b200_batch_create.argtypes = [ctypes.c_int32]
@@ -244,6 +262,18 @@ class Engine:
         Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
         return lib().semper_b200_set_global_model(self._h, _p(Hm, _f64p))
 
+    def set_proposal(self, net, learned: bool = True) -> int:
+        """Learned seeding from `net` (a Proposal, kept alive by this engine)."""
+        self._proposal = net
+        return lib().semper_b200_set_proposal(self._h, None if net is None else net._h, 1 if learned else 0)
+
+    def last_learned(self) -> dict:
+        o = np.zeros(18, np.float64)
+        lib().semper_b200_last_learned(self._h, _p(o, _f64p))
+        return {"ran": bool(o[0]), "proposed": bool(o[1]), "kept": bool(o[2]), "pairs": int(o[3]),
+                "inliers": int(o[4]), "anchors": int(o[5]), "err_mean_px": float(o[6]), "err_max_px": float(o[7]),
+                "ms": float(o[8]), "H": o[9:18].reshape(3, 3).copy()}
+
     def set_tma_wait_limit(self, polls: int) -> int:
         return lib().semper_b200_set_tma_wait_limit(self._h, polls)
 
@@ -259,6 +289,70 @@ class Engine:
         lib().semper_b200_last_global_motion(self._h, _p(o, _f64p))
         return {"locked": bool(o[0]), "theta": o[1], "scale": o[2], "t": (o[3], o[4]), "centre": (o[5], o[6]),
                 "peaks": (o[7], o[8]), "H": o[9:].reshape(3, 3).copy()}
+
+
+class Proposal:
+    """The learned seed proposal network (semper_b200_proposal_*): two 64x64
+    patches -> the affine map between them, on BF16 tensor-core kernels."""
+
+    def __init__(self, max_batch: int = 256):
+        self._h = lib().semper_b200_proposal_create(max_batch)
+        if not self._h:
+            raise RuntimeError("semper_b200_proposal_create failed")
+        self.max_batch = max_batch
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h and _lib is not None:
+            _lib.semper_b200_proposal_destroy(h)
+
+    __del__ = close
+
+    @staticmethod
+    def param_count() -> int:
+        return int(lib().semper_b200_proposal_param_count())
+
+    def set_params(self, flat: np.ndarray):
+        f = np.ascontiguousarray(flat, np.float32)
+        _ck(lib().semper_b200_proposal_set_params(self._h, _p(f, _f32p), f.size), "proposal params")
+
+    def get_params(self) -> np.ndarray:
+        f = np.zeros(self.param_count(), np.float32)
+        _ck(lib().semper_b200_proposal_get_params(self._h, _p(f, _f32p), f.size), "proposal params")
+        return f
+
+    def forward(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        out = np.zeros((x.shape[0], 6), np.float32)
+        _ck(lib().semper_b200_proposal_forward(self._h, _p(x, _f32p), x.shape[0], _p(out, _f32p)), "forward")
+        return out
+
+    def gradients(self, x: np.ndarray, target: np.ndarray):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(target, np.float32)
+        g = np.zeros(self.param_count(), np.float32)
+        loss = np.zeros(1, np.float32)
+        _ck(lib().semper_b200_proposal_gradients(self._h, _p(x, _f32p), _p(t, _f32p), x.shape[0], _p(g, _f32p),
+                                                 _p(loss, _f32p)), "gradients")
+        return float(loss[0]), g
+
+    def synth(self, speckle: np.ndarray, cfg, seed: int, batch: int):
+        s = np.ascontiguousarray(speckle, np.uint8)
+        c = np.asarray(cfg, np.float32)
+        x = np.zeros((batch, 64, 64, 2), np.float32)
+        t = np.zeros((batch, 6), np.float32)
+        _ck(lib().semper_b200_proposal_synth(self._h, _p(s, _u8p), s.shape[1], s.shape[0], _p(c, _f32p), seed, batch,
+                                             _p(x, _f32p), _p(t, _f32p)), "synth")
+        return x, t
+
+    def train(self, speckle: np.ndarray, cfg, steps: int, batch: int, lr: float, seed: int) -> np.ndarray:
+        s = np.ascontiguousarray(speckle, np.uint8)
+        c = np.asarray(cfg, np.float32)
+        losses = np.zeros(max(steps, 1), np.float32)
+        _ck(lib().semper_b200_proposal_train(self._h, _p(s, _u8p), s.shape[1], s.shape[0], _p(c, _f32p), steps, batch,
+                                             lr, seed, _p(losses, _f32p)), "train")
+        return losses[:steps]
 
 
 class Batch:

@@ -129,25 +129,28 @@ def test_cancel_during_frame():
     assert ia.reference_frame == ib.reference_frame
 
 
-def strip_sequence(n=320, frames=12, seed=41, speed=1.6, x0=150, width=14):
+def occluder_sequence(n=320, frames=12, seed=41, speed=2.0):
     """Material translating and stretching under a stationary, textureless
-    band: subsets that overlap the band cannot be matched, so their nodes
-    coast on fitted planes while the band covers them and, once past it, are
-    confirmed only by direct matches of their anchors (cut where they were
-    last clean)."""
+    occluder that appears small (frames 2-3), grows (frames 4-7) and goes.
+    Nodes beside the small one get anchors (a gap within reach), coast on
+    fitted planes while the large one covers them, and when it goes are
+    confirmed only by direct matches of those anchors."""
     ref = sb.speckle(n, n, seed)
     out = []
     for t in range(1, frames + 1):
-        w = sb.warp_block(cx=n / 2, cy=n / 2, u0=speed * t, v0=-0.3 * t, a=(0.002 * t, 0.0, 0.0, -0.001 * t))
+        w = sb.warp_block(cx=n / 2, cy=n / 2, u0=speed * t, v0=-0.5 * t, a=(0.002 * t, 0.0, 0.0, -0.001 * t))
         f = sb.speckle(n, n, seed, w, 1.0, 300 + t)
-        f[:, x0:x0 + width] = 128
+        if 2 <= t <= 3:
+            f[148:172, 148:172] = 128
+        if 4 <= t <= 7:
+            f[112:208, 112:208] = 128
         out.append(f)
     return ref, out
 
 
 @pytest.mark.parametrize("interval", [1, 2])
 def test_coasting_and_anchor_matches_match_restatement(interval):
-    ref, frames = strip_sequence()
+    ref, frames = occluder_sequence()
     dev = sb.Incremental()
     ora = oracle.IncrementalOracle()
     assert dev.init(ref, sb.params((16, 16, 288, 288), 8, 21, 21), interval) == 0
