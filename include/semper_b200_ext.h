@@ -148,6 +148,17 @@ SEMPER_C_API int semper_b200_proposal_train(semper_b200_proposal* p, const uint8
                                             const float cfg[6], int32_t steps, int32_t batch, float lr,
                                             uint64_t seed, float* losses);
 
+/* Predictions for patch pairs cut from two w x h u8 frames (host memory,
+   packed rows) at box factor f: pair k's first patch is the f x f box average
+   of `ref` around (maps[8k], maps[8k+1]); its second samples `def`
+   bilinearly at x' = A X + b for each sample X of the first, with
+   A = [[maps[8k+2], maps[8k+3]], [maps[8k+4], maps[8k+5]]] and
+   b = (maps[8k+6], maps[8k+7]); pixels outside the frame read its nearest
+   edge. out [batch][6] is the residual map the network sees between them. */
+SEMPER_C_API int semper_b200_proposal_predict_warped(semper_b200_proposal* p, const uint8_t* ref,
+                                                     const uint8_t* def, int32_t w, int32_t h, const float* maps,
+                                                     int32_t batch, int32_t f, float* out);
+
 /* Learned seeding on an engine handle: with a proposal network (NULL: none)
    and learned != 0, a run with no model set proposes its global model from
    the network's predictions on patch pairs of the reference and the

@@ -363,12 +363,46 @@ struct Engine::Impl {
         if (++t.trials >= kTuneTrials) t.best = t.t[1] < t.t[0] ? 1 : 0;
     }
 
-    // The learned proposal of the global model: the network's predictions on
-    // patch pairs (box factor 4, 256 px a side), first five pairs at the ROI
-    // centre (the same place in both frames) whose median affine map places
-    // a 6 x 6 grid of pairs over the central 70 % of the ROI, then a
-    // homography fitted to where that grid's patch origins land (DLT with an
-    // inlier refit at 6 px). False when the fit fails.
+    // The learned proposal of the global model, from the network's
+    // predictions on patch pairs (box factor 4, 256 px a side):
+    // 1. five pairs at the ROI centre, three rounds: each round samples the
+    //    deformed patch through the current estimate of the map, the network
+    //    predicts what is left of the motion, and the map takes it on; the
+    //    estimate is the entry-wise median over the pairs;
+    // 2. a 6 x 6 grid of pairs over the central 70 % of the ROI, sampled
+    //    through that estimate, whose predicted residuals say where each
+    //    pair's origin lands;
+    // 3. a homography fitted to those landings (DLT with an inlier refit at
+    //    6 px). False when the fit fails or keeps fewer than 8 pairs.
+    struct Affine {
+        double a00 = 1, a01 = 0, a10 = 0, a11 = 1, bx = 0, by = 0;
+    };
+    // T o E, with E the network's output for a pair whose patches share the
+    // origin (ox, oy): E(X) = o + f t + A_r (X - o).
+    static Affine compose(const Affine& T, const float* o6, double ox, double oy, int f) {
+        const double r00 = 1.0 + o6[0], r01 = o6[1], r10 = o6[2], r11 = 1.0 + o6[3];
+        const double ex = ox + f * dic::kPpTScale * o6[4] - (r00 * ox + r01 * oy);
+        const double ey = oy + f * dic::kPpTScale * o6[5] - (r10 * ox + r11 * oy);
+        Affine C;
+        C.a00 = T.a00 * r00 + T.a01 * r10;
+        C.a01 = T.a00 * r01 + T.a01 * r11;
+        C.a10 = T.a10 * r00 + T.a11 * r10;
+        C.a11 = T.a10 * r01 + T.a11 * r11;
+        C.bx = T.a00 * ex + T.a01 * ey + T.bx;
+        C.by = T.a10 * ex + T.a11 * ey + T.by;
+        return C;
+    }
+    static void map_of(const Affine& T, float cx, float cy, float* m) {
+        m[0] = cx;
+        m[1] = cy;
+        m[2] = (float)T.a00;
+        m[3] = (float)T.a01;
+        m[4] = (float)T.a10;
+        m[5] = (float)T.a11;
+        m[6] = (float)T.bx;
+        m[7] = (float)T.by;
+    }
+
     bool learned_model(const Params& params, const uint8_t* d_def, double H[9]) {
         LearnedSeed& L = E.last_learned_;
         L = LearnedSeed{};
@@ -382,53 +416,46 @@ struct Engine::Impl {
         check(cudaEventRecord(e0, st), "event");
         const int cx = params.rect_x + params.rect_w / 2, cy = params.rect_y + params.rect_h / 2;
         const int off[5][2] = {{0, 0}, {24, 0}, {-24, 0}, {0, 24}, {0, -24}};
-        float c1[5 * 4], o1[5 * 6];
-        for (int k = 0; k < 5; ++k) {
-            c1[4 * k] = c1[4 * k + 2] = (float)(cx + off[k][0]);
-            c1[4 * k + 1] = c1[4 * k + 3] = (float)(cy + off[k][1]);
+        Affine T;
+        float maps[36 * 8], o6[36 * 6];
+        for (int round = 0; round < 3; ++round) {
+            for (int k = 0; k < 5; ++k) map_of(T, (float)(cx + off[k][0]), (float)(cy + off[k][1]), maps + 8 * k);
+            net.predict_warped(rGray.p, d_def, W, Hh, W, maps, 5, f, o6, st);
+            std::vector<double> comp[6];
+            for (int k = 0; k < 5; ++k) {
+                const Affine C = compose(T, o6 + 6 * k, maps[8 * k] - 0.5, maps[8 * k + 1] - 0.5, f);
+                const double v[6] = {C.a00, C.a01, C.a10, C.a11, C.bx, C.by};
+                for (int i = 0; i < 6; ++i) comp[i].push_back(v[i]);
+            }
+            double m[6];
+            for (int i = 0; i < 6; ++i) {
+                std::sort(comp[i].begin(), comp[i].end());
+                m[i] = comp[i][2];
+            }
+            T = Affine{m[0], m[1], m[2], m[3], m[4], m[5]};
         }
-        net.predict_device(rGray.p, d_def, W, Hh, W, c1, 5, f, o1, st);
-        // x' = A x + b per pair, about its origin c - 0.5; the median entry-wise
-        std::vector<double> comp[6];
-        for (int k = 0; k < 5; ++k) {
-            const double a00 = 1.0 + o1[6 * k], a01 = o1[6 * k + 1], a10 = o1[6 * k + 2], a11 = 1.0 + o1[6 * k + 3];
-            const double tx = f * dic::kPpTScale * o1[6 * k + 4], ty = f * dic::kPpTScale * o1[6 * k + 5];
-            const double ox = c1[4 * k] - 0.5, oy = c1[4 * k + 1] - 0.5;
-            comp[0].push_back(a00);
-            comp[1].push_back(a01);
-            comp[2].push_back(a10);
-            comp[3].push_back(a11);
-            comp[4].push_back(ox + tx - (a00 * ox + a01 * oy));
-            comp[5].push_back(oy + ty - (a10 * ox + a11 * oy));
-        }
-        double m[6];
-        for (int i = 0; i < 6; ++i) {
-            std::sort(comp[i].begin(), comp[i].end());
-            m[i] = comp[i][2];
-        }
-        // the grid of pairs, each placed by the centre's map
+        // the grid of pairs, sampled through the centre's estimate
         constexpr int G = 6;
-        std::vector<float> c2;
-        std::vector<semper_geom::Pt> rp, dp;
+        int K = 0;
         for (int j = 0; j < G; ++j)
             for (int i = 0; i < G; ++i) {
                 const int rx = params.rect_x + (int)(params.rect_w * (0.15 + 0.7 * (i + 0.5) / G));
                 const int ry = params.rect_y + (int)(params.rect_h * (0.15 + 0.7 * (j + 0.5) / G));
-                const double X = rx - 0.5, Y = ry - 0.5;
-                const double px = m[0] * X + m[1] * Y + m[4] + 0.5, py = m[2] * X + m[3] * Y + m[5] + 0.5;
+                const double px = T.a00 * rx + T.a01 * ry + T.bx, py = T.a10 * rx + T.a11 * ry + T.by;
                 if (!(px > 0.0 && py > 0.0 && px < W - 1 && py < Hh - 1)) continue;
-                c2.insert(c2.end(), {(float)rx, (float)ry, (float)std::lround(px), (float)std::lround(py)});
+                map_of(T, (float)rx, (float)ry, maps + 8 * K);
+                ++K;
             }
-        const int K = (int)c2.size() / 4;
-        L.pairs = K;
+        L.pairs = 15 + K;
         bool ok = false;
-        if (K >= 8 && K <= net.max_batch()) {
-            std::vector<float> o2((size_t)K * 6);
-            net.predict_device(rGray.p, d_def, W, Hh, W, c2.data(), K, f, o2.data(), st);
+        if (K >= 8) {
+            net.predict_warped(rGray.p, d_def, W, Hh, W, maps, K, f, o6, st);
+            std::vector<semper_geom::Pt> rp, dp;
             for (int k = 0; k < K; ++k) {
-                rp.push_back({c2[4 * k] - 0.5, c2[4 * k + 1] - 0.5});
-                dp.push_back({c2[4 * k + 2] - 0.5 + f * dic::kPpTScale * o2[6 * k + 4],
-                              c2[4 * k + 3] - 0.5 + f * dic::kPpTScale * o2[6 * k + 5]});
+                const double ox = maps[8 * k] - 0.5, oy = maps[8 * k + 1] - 0.5;
+                const Affine C = compose(T, o6 + 6 * k, ox, oy, f);
+                rp.push_back({ox, oy});
+                dp.push_back({C.a00 * ox + C.a01 * oy + C.bx, C.a10 * ox + C.a11 * oy + C.by});
             }
             ok = semper_geom::fit_homography(rp, dp, 6.0, H);
             if (ok) {
@@ -446,7 +473,7 @@ struct Engine::Impl {
         cudaEventElapsedTime(&L.ms, e0, e1);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        E.times_.launches += 2 * 14;
+        E.times_.launches += 4 * 14;
         L.proposed = ok;
         if (ok) std::copy(H, H + 9, L.H);
         return ok;

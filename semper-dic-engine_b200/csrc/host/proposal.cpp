@@ -155,4 +155,26 @@ void ProposalNet::predict_device(const uint8_t* d_ref, const uint8_t* d_def, int
     check(cudaStreamSynchronize(st), "sync");
 }
 
+void ProposalNet::predict_warped(const uint8_t* d_ref, const uint8_t* d_def, int W, int H, int pitch,
+                                 const float* maps, int K, int f, float* out, cudaStream_t st) {
+    if (K <= 0 || K > max_batch_) throw std::invalid_argument("proposal: batch");
+    if (W < 2 || H < 2 || pitch < W || f < 1 || f > 16) throw std::invalid_argument("proposal: frame or factor");
+    centres_.ensure(std::max(centres_.n, (size_t)K * 8));
+    check(cudaMemcpyAsync(centres_.p, maps, (size_t)K * 32, cudaMemcpyHostToDevice, st), "H2D maps");
+    check(dic::pp_cut_warped(d_ref, d_def, W, H, pitch, centres_.p, K, f, w_.act[0], st), "cut warped");
+    check(dic::pp_forward(params_.p, w_, K, st), "proposal forward");
+    check(cudaMemcpyAsync(out, w_.out, (size_t)K * 6 * 4, cudaMemcpyDeviceToHost, st), "D2H out");
+    check(cudaStreamSynchronize(st), "sync");
+}
+
+void ProposalNet::predict_warped_host(const uint8_t* ref, const uint8_t* def, int W, int H, const float* maps, int K,
+                                      int f, float* out) {
+    if (W < 2 || H < 2) throw std::invalid_argument("proposal: frame size");
+    const size_t n = (size_t)W * H;
+    frames_.ensure(std::max(frames_.n, 2 * n));
+    check(cudaMemcpyAsync(frames_.p, ref, n, cudaMemcpyHostToDevice, st_), "H2D ref");
+    check(cudaMemcpyAsync(frames_.p + n, def, n, cudaMemcpyHostToDevice, st_), "H2D def");
+    predict_warped(frames_.p, frames_.p + n, W, H, W, maps, K, f, out, st_);
+}
+
 }  // namespace semper_b200

@@ -45,12 +45,21 @@ public:
     void predict_device(const uint8_t* d_ref, const uint8_t* d_def, int W, int H, int pitch, const float* centres,
                         int K, int f, float* out, cudaStream_t st);
 
+    // The same with each pair's second patch sampled through an affine map
+    // (maps host [K, 8]: ref centre x, y, then a00 a01 a10 a11 bx by).
+    void predict_warped(const uint8_t* d_ref, const uint8_t* d_def, int W, int H, int pitch, const float* maps,
+                        int K, int f, float* out, cudaStream_t st);
+    // predict_warped on u8 frames in host memory (W x H, packed rows), on the
+    // network's own stream.
+    void predict_warped_host(const uint8_t* ref, const uint8_t* def, int W, int H, const float* maps, int K, int f,
+                             float* out);
+
 private:
     void upload_speckle(const uint8_t* speckle, int W, int H);
     int max_batch_;
     cudaStream_t st_ = nullptr;
     DevBuf<float> params_, grads_, m_, v_, target_, centres_, speckle_f_;
-    DevBuf<unsigned char> work_;
+    DevBuf<unsigned char> work_, frames_;
     dic::PpWork w_;
     int adam_t_ = 0;
 };

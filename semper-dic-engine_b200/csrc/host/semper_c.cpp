@@ -466,6 +466,20 @@ SEMPER_C_API int semper_b200_proposal_train(semper_b200_proposal* p, const uint8
     });
 }
 
+SEMPER_C_API int semper_b200_proposal_predict_warped(semper_b200_proposal* p, const uint8_t* ref,
+                                                     const uint8_t* def, int32_t w, int32_t h, const float* maps,
+                                                     int32_t batch, int32_t f, float* out) {
+    if (!p || !ref || !def || !maps || !out || w < 2 || h < 2 || f < 1 || f > 16 || batch <= 0 ||
+        batch > p->net->max_batch())
+        return SEMPER_ERR_INIT;
+    for (int32_t k = 0; k < 8 * batch; ++k)
+        if (!std::isfinite(maps[k]) || (k % 8 < 2 && std::fabs(maps[k]) > 1e7f)) return SEMPER_ERR_INIT;
+    return guarded(SEMPER_ERR_INIT, [&] {
+        p->net->predict_warped_host(ref, def, w, h, maps, batch, f, out);
+        return 0;
+    });
+}
+
 SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_proposal* p, int learned) {
     if (eng == nullptr) return SEMPER_ERR_INIT;
     HandleCall call(eng->busy);

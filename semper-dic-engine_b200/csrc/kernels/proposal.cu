@@ -446,6 +446,43 @@ __global__ void __launch_bounds__(256) cut_kernel(const uint8_t* __restrict__ re
     normalise_store(v, x + (size_t)k * 8192);
 }
 
+__device__ __forceinline__ float bilinear_u8(const uint8_t* im, int W, int H, int pitch, float x, float y) {
+    x = fminf(fmaxf(x, 0.0f), (float)(W - 1));
+    y = fminf(fmaxf(y, 0.0f), (float)(H - 1));
+    const int x0 = min((int)x, W - 2), y0 = min((int)y, H - 2);
+    const float fx = x - (float)x0, fy = y - (float)y0;
+    const uint8_t* r0 = im + (size_t)y0 * pitch + x0;
+    const uint8_t* r1 = r0 + pitch;
+    return (1.0f - fy) * ((1.0f - fx) * r0[0] + fx * r0[1]) + fy * ((1.0f - fx) * r1[0] + fx * r1[1]);
+}
+
+__global__ void __launch_bounds__(256) cut_warped_kernel(const uint8_t* __restrict__ ref,
+                                                         const uint8_t* __restrict__ def, int W, int H, int pitch,
+                                                         const float* __restrict__ maps, int f, uint16_t* x) {
+    extern __shared__ float vbuf[];
+    float(*v)[4096] = reinterpret_cast<float(*)[4096]>(vbuf);
+    const int k = blockIdx.x;
+    const float* m = maps + 8 * k;
+    const int ax = (int)m[0], ay = (int)m[1];
+    const float inv_f2 = 1.0f / (float)(f * f);
+    for (int i = threadIdx.x; i < 4096; i += 256) {
+        const int u = i & 63, w = i >> 6;
+        float r = 0.0f, d = 0.0f;
+        for (int sj = 0; sj < f; ++sj)
+            for (int si = 0; si < f; ++si) {
+                const int X = ax + f * (u - 32) + si, Y = ay + f * (w - 32) + sj;
+                r += px_clamped(ref, W, H, pitch, X, Y);
+                const float xd = m[2] * (float)X + m[3] * (float)Y + m[6];
+                const float yd = m[4] * (float)X + m[5] * (float)Y + m[7];
+                d += bilinear_u8(def, W, H, pitch, xd, yd);
+            }
+        v[0][i] = r * inv_f2;
+        v[1][i] = d * inv_f2;
+    }
+    __syncthreads();
+    normalise_store(v, x + (size_t)k * 8192);
+}
+
 inline unsigned nblocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -581,6 +618,16 @@ cudaError_t pp_cut_pairs(const uint8_t* ref, const uint8_t* def, int W, int H, i
     cudaError_t e = cudaFuncSetAttribute(cut_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 4096 * 4);
     if (e != cudaSuccess) return e;
     cut_kernel<<<B, 256, 2 * 4096 * 4, st>>>(ref, def, W, H, pitch, centres, f, x);
+    return cudaGetLastError();
+}
+
+cudaError_t pp_cut_warped(const uint8_t* ref, const uint8_t* def, int W, int H, int pitch, const float* maps, int B,
+                          int f, uint16_t* x, cudaStream_t st) {
+    if (B <= 0) return cudaSuccess;
+    cudaError_t e =
+        cudaFuncSetAttribute(cut_warped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 4096 * 4);
+    if (e != cudaSuccess) return e;
+    cut_warped_kernel<<<B, 256, 2 * 4096 * 4, st>>>(ref, def, W, H, pitch, maps, f, x);
     return cudaGetLastError();
 }
 

@@ -62,6 +62,14 @@ cudaError_t pp_adam(float* params, const float* grads, float* m, float* v, size_
 cudaError_t pp_cut_pairs(const uint8_t* ref, const uint8_t* def, int W, int H, int pitch, const float* centres,
                          int B, int f, uint16_t* x, cudaStream_t st);
 
+// The same with the second patch sampled through an affine map: pair k's
+// second patch takes, for each sample X of its first patch (the f x f pixels
+// around centre (ax_k, ay_k)), `def` at x' = A_k X + b_k (bilinear, clamped
+// to the frame); maps [B][8] = ax, ay, a00, a01, a10, a11, bx, by. With the
+// map the true one, the two patches show the same material.
+cudaError_t pp_cut_warped(const uint8_t* ref, const uint8_t* def, int W, int H, int pitch, const float* maps, int B,
+                          int f, uint16_t* x, cudaStream_t st);
+
 // Synthetic training pairs from a float speckle image S (W x H): pair k gets
 // a random centre c, rotation, small stretch and shear and translation t; its
 // first patch is S box-averaged by f around c, its second the warped image

@@ -46,6 +46,7 @@ EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b20
                "semper_b200_proposal_create", "semper_b200_proposal_destroy", "semper_b200_proposal_param_count",
                "semper_b200_proposal_set_params", "semper_b200_proposal_get_params", "semper_b200_proposal_forward",
                "semper_b200_proposal_gradients", "semper_b200_proposal_synth", "semper_b200_proposal_train",
+               "semper_b200_proposal_predict_warped",
                "semper_b200_set_proposal", "semper_b200_last_learned"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
@@ -126,6 +127,8 @@ def lib():
                                                  ctypes.c_int32, _f32p, _f32p]
         L.semper_b200_proposal_train.argtypes = [_vp, _u8p, ctypes.c_int32, ctypes.c_int32, _f32p, ctypes.c_int32,
                                                  ctypes.c_int32, ctypes.c_float, ctypes.c_uint64, _f32p]
+        L.semper_b200_proposal_predict_warped.argtypes = [_vp, _u8p, _u8p, ctypes.c_int32, ctypes.c_int32, _f32p,
+                                                          ctypes.c_int32, ctypes.c_int32, _f32p]
         L.semper_b200_set_proposal.argtypes = [_vp, _vp, ctypes.c_int]
         L.semper_b200_last_learned.argtypes = [_vp, _f64p]
         L.semper_b200_set_tma_wait_limit.argtypes = [_vp, ctypes.c_int]
@@ -353,6 +356,18 @@ class Proposal:
         _ck(lib().semper_b200_proposal_train(self._h, _p(s, _u8p), s.shape[1], s.shape[0], _p(c, _f32p), steps, batch,
                                              lr, seed, _p(losses, _f32p)), "train")
         return losses[:steps]
+
+    def predict_warped(self, ref: np.ndarray, dfm: np.ndarray, maps: np.ndarray, f: int) -> np.ndarray:
+        """Residual maps [K, 6] for pairs cut from two u8 frames, the second
+        patch of each sampled through maps[k] = (cx, cy, a00, a01, a10, a11,
+        bx, by) (semper_b200_proposal_predict_warped)."""
+        r = np.ascontiguousarray(ref, np.uint8)
+        d = np.ascontiguousarray(dfm, np.uint8)
+        m = np.ascontiguousarray(maps, np.float32).reshape(-1, 8)
+        out = np.zeros((m.shape[0], 6), np.float32)
+        _ck(lib().semper_b200_proposal_predict_warped(self._h, _p(r, _u8p), _p(d, _u8p), r.shape[1], r.shape[0],
+                                                      _p(m, _f32p), m.shape[0], f, _p(out, _f32p)), "predict_warped")
+        return out
 
 
 class Batch:
