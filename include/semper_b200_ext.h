@@ -175,6 +175,12 @@ SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_propos
    [9..17] the proposed homography (row-major). Returns 0, or -3. */
 SEMPER_C_API int semper_b200_last_learned(semper_engine* eng, double out[18]);
 
+/* The last run's per-anchor guesses of the learned seeding: for every node of
+   the anchor lattice (row-major), the displacement (u, v) the network put
+   forward under the proposed model, NaN where none. Returns the node count n
+   (the guesses are copied when capacity >= 2n floats), or -3. */
+SEMPER_C_API int semper_b200_learned_guesses(semper_engine* eng, float* uv, int32_t capacity);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

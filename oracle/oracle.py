@@ -52,6 +52,8 @@ def lib(kind: str = "contract"):
         L.oracle_set_reference.argtypes = [ctypes.c_void_p, _u8p, ctypes.c_int, ctypes.c_int, _u8p]
         L.oracle_run.argtypes = [ctypes.c_void_p, _u8p, _u8p, _i32p, _f32p, ctypes.c_int, _f32p,
                                  ctypes.c_int, _f64p]
+        L.oracle_run_guided.argtypes = [ctypes.c_void_p, _u8p, _u8p, _i32p, _f32p, ctypes.c_int, _f32p,
+                                        ctypes.c_int, _f64p, _f32p, ctypes.c_int]
         L.oracle_run_capture.argtypes = [ctypes.c_void_p, _u8p, _u8p, _i32p, _f32p, ctypes.c_int,
                                          _f32p, ctypes.c_int, _f64p, _f32p, _i32p, ctypes.c_int]
         L.oracle_prepare.argtypes = [_u8p, ctypes.c_int, ctypes.c_int, _u8p, _f32p, _f32p, _f32p]
@@ -117,7 +119,9 @@ class Oracle:
         return self._L.oracle_set_reference(self._h, _p(gray, _u8p), gray.shape[1], gray.shape[0], _p(m, _u8p))
 
     def run(self, deformed: np.ndarray, params, capacity: int | None = None, mask=None, model_h=None,
-            metrics_len: int = 24, capture: bool = False):
+            metrics_len: int = 24, capture: bool = False, anchor_uv=None):
+        """run_full_field. anchor_uv ([n][2] float32, NaN for none): per
+        anchor-lattice node displacement guesses under model_h."""
         d = np.ascontiguousarray(deformed, np.uint8)
         m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
         p = np.asarray(params, np.int32)
@@ -127,6 +131,13 @@ class Oracle:
         out = np.zeros(max(capacity, 1), np.float32)
         met = np.zeros(max(metrics_len, 1), np.float32)
         H = None if model_h is None else np.ascontiguousarray(model_h, np.float64).reshape(9)
+        if anchor_uv is not None:
+            g = np.ascontiguousarray(anchor_uv, np.float32).reshape(-1, 2)
+            rc = self._L.oracle_run_guided(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
+                                           capacity, _p(met, _f32p), metrics_len, _p(H, _f64p), _p(g, _f32p),
+                                           g.shape[0])
+            pts = out[: max(rc, 0) * 8].reshape(-1, 8).copy()
+            return rc, pts, met[:metrics_len].copy()
         if not capture:
             rc = self._L.oracle_run(self._h, _p(d, _u8p), _p(m, _u8p), _p(p, _i32p), _p(out, _f32p),
                                   capacity, _p(met, _f32p), metrics_len, _p(H, _f64p))

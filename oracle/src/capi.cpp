@@ -90,6 +90,21 @@ int oracle_run(void* p, const uint8_t* def, const uint8_t* mask, const int32_t* 
     return run_full_field<float>(H->c32, def, mask, q, out, cap, metrics, mlen, model_H);
 }
 
+// oracle_run with per-anchor displacement guesses under the model: anchor_uv
+// [anchor_n][2] in the anchor lattice's row-major order (NaN: none), used when
+// anchor_n equals the lattice's size.
+int oracle_run_guided(void* p, const uint8_t* def, const uint8_t* mask, const int32_t* params, float* out,
+                      int cap, float* metrics, int mlen, const double* model_H, const float* anchor_uv,
+                      int anchor_n) {
+    Handle* H = static_cast<Handle*>(p);
+    const Params q = to_params(params);
+    if (H->fp64)
+        return run_full_field<double>(H->c64, def, mask, q, out, cap, metrics, mlen, model_H, nullptr, nullptr,
+                                      anchor_uv, anchor_n);
+    return run_full_field<float>(H->c32, def, mask, q, out, cap, metrics, mlen, model_H, nullptr, nullptr,
+                                 anchor_uv, anchor_n);
+}
+
 // Per-node raw results of the last kind of solve (Capture), for the device
 // pipeline's intermediate parity checks: per grid node
 // [u v ux uy vx vy corr] + [solved mesh icgn_iters used_simplex].

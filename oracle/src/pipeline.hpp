@@ -248,7 +248,8 @@ inline PackOut pack_field(const std::vector<GridPoint>& grid, int gridW, int gri
 template <class T>
 int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* mask, Params params,
                    float* out, int capacity, float* metrics, int metrics_len, const double* model_H,
-                   Capture* capture = nullptr, Image<T>* keep_def = nullptr) {
+                   Capture* capture = nullptr, Image<T>* keep_def = nullptr, const float* anchor_uv = nullptr,
+                   int anchor_n = 0) {
     using clk = std::chrono::high_resolution_clock;
     auto ms_since = [](clk::time_point t) { return std::chrono::duration<double, std::milli>(clk::now() - t).count(); };
     const auto t_total = clk::now();
@@ -407,6 +408,12 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
             const int rx = params.rect_x + gx * params.step, ry = params.rect_y + gy * params.step;
             float gs[6] = {globalU, globalV, 0, 0, 0, 0};
             if (sim && !model_at(rx, ry, gs)) { gs[0] = globalU; gs[1] = globalV; gs[2] = gs[3] = gs[4] = gs[5] = 0; }
+            // a per-anchor displacement guess under the model (the device's
+            // learned seeding hands its network's guesses over here)
+            if (sim && anchor_n == LW * LH && std::isfinite(anchor_uv[2 * i]) && std::isfinite(anchor_uv[2 * i + 1])) {
+                gs[0] = anchor_uv[2 * i];
+                gs[1] = anchor_uv[2 * i + 1];
+            }
             T g[6];
             for (int k = 0; k < 6; ++k) g[k] = (T)gs[k];
             Engine<T> eng = make_engine();

@@ -17,6 +17,7 @@
 #include "proposal.hpp"
 
 #include <algorithm>
+#include <limits>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -364,16 +365,21 @@ struct Engine::Impl {
     }
 
     // The learned proposal of the global model, from the network's
-    // predictions on patch pairs (box factor 4, 256 px a side):
-    // 1. five pairs at the ROI centre, three rounds: each round samples the
-    //    deformed patch through the current estimate of the map, the network
-    //    predicts what is left of the motion, and the map takes it on; the
-    //    estimate is the entry-wise median over the pairs;
-    // 2. a 6 x 6 grid of pairs over the central 70 % of the ROI, sampled
-    //    through that estimate, whose predicted residuals say where each
-    //    pair's origin lands;
-    // 3. a homography fitted to those landings (DLT with an inlier refit at
-    //    6 px). False when the fit fails or keeps fewer than 8 pairs.
+    // predictions on patch pairs (64 x 64 patches box-averaged by f):
+    // 1. the rotation about the ROI centre, four rounds at f = 4, 4, 4, 2 over
+    //    nine pairs (the centre and eight at 48 px around it): each round
+    //    samples the deformed patches through the current estimate, the
+    //    network predicts what is left of the motion, every pair's map takes
+    //    its prediction on, and the estimate becomes the rotation by the
+    //    pairs' circular median angle that lands the centre on their median
+    //    landing (a pure rotation, so that no stray shear or scale carries
+    //    the next round outside the motions the network was trained on);
+    // 2. a 6 x 6 grid of pairs over the central 70 % of the ROI, started from
+    //    that rotation, three rounds at f = 4, 2, 1, each pair's own affine
+    //    map refined by the network's prediction;
+    // 3. a homography fitted to where the pairs' origins land (DLT with an
+    //    inlier refit at 6 px). False when the fit fails or keeps fewer than
+    //    8 pairs.
     struct Affine {
         double a00 = 1, a01 = 0, a10 = 0, a11 = 1, bx = 0, by = 0;
     };
@@ -403,80 +409,164 @@ struct Engine::Impl {
         m[7] = (float)T.by;
     }
 
+    static Affine rotation_landing(const std::vector<Affine>& C, double ox, double oy) {
+        const size_t n = C.size();
+        std::vector<double> th(n), lx(n), ly(n);
+        for (size_t k = 0; k < n; ++k) {
+            th[k] = std::atan2(C[k].a10 - C[k].a01, C[k].a00 + C[k].a11);
+            lx[k] = C[k].a00 * ox + C[k].a01 * oy + C[k].bx;
+            ly[k] = C[k].a10 * ox + C[k].a11 * oy + C[k].by;
+        }
+        // circular median: the angle with the least summed distance to the others
+        size_t best = 0;
+        double best_d = 0.0;
+        for (size_t k = 0; k < n; ++k) {
+            double d = 0.0;
+            for (size_t j = 0; j < n; ++j) d += std::fabs(std::remainder(th[k] - th[j], 2.0 * M_PI));
+            if (k == 0 || d < best_d) {
+                best = k;
+                best_d = d;
+            }
+        }
+        std::nth_element(lx.begin(), lx.begin() + n / 2, lx.end());
+        std::nth_element(ly.begin(), ly.begin() + n / 2, ly.end());
+        const double c = std::cos(th[best]), s = std::sin(th[best]);
+        Affine T;
+        T.a00 = c;
+        T.a01 = -s;
+        T.a10 = s;
+        T.a11 = c;
+        T.bx = lx[n / 2] - (c * ox - s * oy);
+        T.by = ly[n / 2] - (s * ox + c * oy);
+        return T;
+    }
+
     bool learned_model(const Params& params, const uint8_t* d_def, double H[9]) {
         LearnedSeed& L = E.last_learned_;
         L = LearnedSeed{};
         L.ran = true;
         ProposalNet& net = *E.proposal_;
         cudaStream_t st = E.stream_;
-        const int W = E.W_, Hh = E.H_, f = 4;
+        const int W = E.W_, Hh = E.H_;
         cudaEvent_t e0, e1;
         check(cudaEventCreate(&e0), "event");
         check(cudaEventCreate(&e1), "event");
         check(cudaEventRecord(e0, st), "event");
         const int cx = params.rect_x + params.rect_w / 2, cy = params.rect_y + params.rect_h / 2;
-        const int off[5][2] = {{0, 0}, {24, 0}, {-24, 0}, {0, 24}, {0, -24}};
-        Affine T;
-        float maps[36 * 8], o6[36 * 6];
-        for (int round = 0; round < 3; ++round) {
-            for (int k = 0; k < 5; ++k) map_of(T, (float)(cx + off[k][0]), (float)(cy + off[k][1]), maps + 8 * k);
-            net.predict_warped(rGray.p, d_def, W, Hh, W, maps, 5, f, o6, st);
-            std::vector<double> comp[6];
-            for (int k = 0; k < 5; ++k) {
-                const Affine C = compose(T, o6 + 6 * k, maps[8 * k] - 0.5, maps[8 * k + 1] - 0.5, f);
-                const double v[6] = {C.a00, C.a01, C.a10, C.a11, C.bx, C.by};
-                for (int i = 0; i < 6; ++i) comp[i].push_back(v[i]);
-            }
-            double m[6];
-            for (int i = 0; i < 6; ++i) {
-                std::sort(comp[i].begin(), comp[i].end());
-                m[i] = comp[i][2];
-            }
-            T = Affine{m[0], m[1], m[2], m[3], m[4], m[5]};
+        const double ox = cx - 0.5, oy = cy - 0.5;
+        constexpr int kRing = 9, G = 6;
+        int px[G * G], py[G * G];
+        px[0] = cx;
+        py[0] = cy;
+        for (int k = 1; k < kRing; ++k) {
+            const double a = (k - 1) * (M_PI / 4.0);
+            px[k] = cx + (int)std::lround(48.0 * std::cos(a));
+            py[k] = cy + (int)std::lround(48.0 * std::sin(a));
         }
-        // the grid of pairs, sampled through the centre's estimate
-        constexpr int G = 6;
-        int K = 0;
+        float maps[G * G * 8], o6[G * G * 6];
+        Affine T;
+        std::vector<Affine> C(kRing);
+        for (const int f : {4, 4, 4, 2}) {
+            for (int k = 0; k < kRing; ++k) map_of(T, (float)px[k], (float)py[k], maps + 8 * k);
+            net.predict_warped(rGray.p, d_def, W, Hh, W, maps, kRing, f, o6, st);
+            for (int k = 0; k < kRing; ++k) C[k] = compose(T, o6 + 6 * k, px[k] - 0.5, py[k] - 0.5, f);
+            T = rotation_landing(C, ox, oy);
+            L.pairs += kRing;
+        }
+        constexpr int K = G * G;
+        std::vector<Affine> Tg(K, T);
         for (int j = 0; j < G; ++j)
             for (int i = 0; i < G; ++i) {
-                const int rx = params.rect_x + (int)(params.rect_w * (0.15 + 0.7 * (i + 0.5) / G));
-                const int ry = params.rect_y + (int)(params.rect_h * (0.15 + 0.7 * (j + 0.5) / G));
-                const double px = T.a00 * rx + T.a01 * ry + T.bx, py = T.a10 * rx + T.a11 * ry + T.by;
-                if (!(px > 0.0 && py > 0.0 && px < W - 1 && py < Hh - 1)) continue;
-                map_of(T, (float)rx, (float)ry, maps + 8 * K);
-                ++K;
+                px[j * G + i] = params.rect_x + (int)(params.rect_w * (0.15 + 0.7 * (i + 0.5) / G));
+                py[j * G + i] = params.rect_y + (int)(params.rect_h * (0.15 + 0.7 * (j + 0.5) / G));
             }
-        L.pairs = 15 + K;
-        bool ok = false;
-        if (K >= 8) {
+        for (const int f : {4, 2, 1}) {
+            for (int k = 0; k < K; ++k) map_of(Tg[k], (float)px[k], (float)py[k], maps + 8 * k);
             net.predict_warped(rGray.p, d_def, W, Hh, W, maps, K, f, o6, st);
-            std::vector<semper_geom::Pt> rp, dp;
-            for (int k = 0; k < K; ++k) {
-                const double ox = maps[8 * k] - 0.5, oy = maps[8 * k + 1] - 0.5;
-                const Affine C = compose(T, o6 + 6 * k, ox, oy, f);
-                rp.push_back({ox, oy});
-                dp.push_back({C.a00 * ox + C.a01 * oy + C.bx, C.a10 * ox + C.a11 * oy + C.by});
+            for (int k = 0; k < K; ++k) Tg[k] = compose(Tg[k], o6 + 6 * k, px[k] - 0.5, py[k] - 0.5, f);
+            L.pairs += K;
+        }
+        std::vector<semper_geom::Pt> rp, dp;
+        for (int k = 0; k < K; ++k) {
+            const double x = px[k] - 0.5, y = py[k] - 0.5;
+            const double X = Tg[k].a00 * x + Tg[k].a01 * y + Tg[k].bx, Y = Tg[k].a10 * x + Tg[k].a11 * y + Tg[k].by;
+            if (!std::isfinite(X) || !std::isfinite(Y)) continue;
+            rp.push_back({x, y});
+            dp.push_back({X, Y});
+        }
+        bool ok = rp.size() >= 8 && semper_geom::fit_homography(rp, dp, 6.0, H);
+        if (ok) {
+            for (size_t k = 0; k < rp.size(); ++k) {
+                double X, Y, J[4];
+                if (semper_geom::homography_at(H, rp[k].x, rp[k].y, X, Y, J) &&
+                    std::hypot(X - dp[k].x, Y - dp[k].y) <= 6.0)
+                    L.inliers++;
             }
-            ok = semper_geom::fit_homography(rp, dp, 6.0, H);
-            if (ok) {
-                for (int k = 0; k < K; ++k) {
-                    double X, Y, J[4];
-                    if (semper_geom::homography_at(H, rp[k].x, rp[k].y, X, Y, J) &&
-                        std::hypot(X - dp[k].x, Y - dp[k].y) <= 6.0)
-                        L.inliers++;
-                }
-                ok = L.inliers >= 8;
-            }
+            ok = L.inliers >= 8;
         }
         check(cudaEventRecord(e1, st), "event");
         check(cudaEventSynchronize(e1), "event");
         cudaEventElapsedTime(&L.ms, e0, e1);
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
-        E.times_.launches += 4 * 14;
+        E.times_.launches += 7 * 14;
         L.proposed = ok;
         if (ok) std::copy(H, H + 9, L.H);
         return ok;
+    }
+
+    // Each anchor's displacement under the proposed model H, refined by the
+    // network: the map starts as H's local affine at the anchor, two rounds
+    // at f = 2 and 1 move it by the network's predictions, and the guess is
+    // where the anchor's pixel lands (the gradients stay H's). One entry per
+    // lattice node, NaN for nodes that are not attempted.
+    std::vector<float> learned_anchor_guesses(const uint8_t* d_def, const double* H, const Params& params,
+                                              const std::vector<int>& lat_x, const std::vector<int>& lat_y,
+                                              const std::vector<uint8_t>& solved, int gW) {
+        ProposalNet& net = *E.proposal_;
+        const int LW = (int)lat_x.size(), LH = (int)lat_y.size(), N = LW * LH;
+        std::vector<float> uv((size_t)2 * N, std::numeric_limits<float>::quiet_NaN());
+        std::vector<int> idx, px, py;
+        std::vector<Affine> Tk;
+        for (int i = 0; i < N; ++i) {
+            const int gx = lat_x[i % LW], gy = lat_y[i / LW];
+            if (solved[(size_t)gy * gW + gx]) continue;
+            const int x = params.rect_x + gx * params.step, y = params.rect_y + gy * params.step;
+            double X, Y, J[4];
+            if (!semper_geom::homography_at(H, x, y, X, Y, J)) continue;
+            Affine T;
+            T.a00 = J[0];
+            T.a01 = J[1];
+            T.a10 = J[2];
+            T.a11 = J[3];
+            T.bx = X - (J[0] * x + J[1] * y);
+            T.by = Y - (J[2] * x + J[3] * y);
+            idx.push_back(i);
+            px.push_back(x);
+            py.push_back(y);
+            Tk.push_back(T);
+        }
+        const int K = (int)idx.size(), B = net.max_batch();
+        std::vector<float> maps((size_t)B * 8), o6((size_t)B * 6);
+        for (const int f : {2, 1}) {
+            for (int k0 = 0; k0 < K; k0 += B) {
+                const int nb = std::min(B, K - k0);
+                for (int k = 0; k < nb; ++k) map_of(Tk[k0 + k], (float)px[k0 + k], (float)py[k0 + k], &maps[8 * k]);
+                net.predict_warped(rGray.p, d_def, E.W_, E.H_, E.W_, maps.data(), nb, f, o6.data(), E.stream_);
+                for (int k = 0; k < nb; ++k)
+                    Tk[k0 + k] = compose(Tk[k0 + k], &o6[6 * k], px[k0 + k] - 0.5, py[k0 + k] - 0.5, f);
+                E.times_.launches += 14;
+                E.last_learned_.pairs += nb;
+            }
+        }
+        for (int k = 0; k < K; ++k) {
+            const double x = px[k], y = py[k];
+            const double X = Tk[k].a00 * x + Tk[k].a01 * y + Tk[k].bx, Y = Tk[k].a10 * x + Tk[k].a11 * y + Tk[k].by;
+            if (!std::isfinite(X) || !std::isfinite(Y)) continue;
+            uv[2 * (size_t)idx[k]] = (float)(X - x);
+            uv[2 * (size_t)idx[k] + 1] = (float)(Y - y);
+        }
+        return uv;
     }
 
     dic::SolveArgs solve_args(int dim, int six) {
@@ -1019,6 +1109,33 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         for (int gy = 0; gy < gH; gy += sy) lat_y.push_back(gy);
         if (lat_y.back() != gH - 1) lat_y.push_back(gH - 1);
         const int LW = (int)lat_x.size(), LH = (int)lat_y.size();
+        // learned seeding: the network's guess per anchor under its model
+        std::vector<float> anchor_uv;
+        bool guided = false;
+        if (learned) {
+            const auto t_g = clk::now();
+            anchor_uv = learned_anchor_guesses(d_def, model_H, params, lat_x, lat_y, solved, gW);
+            // the model refitted to where the anchors land under the guesses,
+            // so that what the keep rule measures against it is the field's own
+            // departure from a homography, not the coarse estimate's error
+            std::vector<semper_geom::Pt> rp, dp;
+            for (int i = 0; i < LW * LH; ++i) {
+                if (!std::isfinite(anchor_uv[2 * (size_t)i]) || !std::isfinite(anchor_uv[2 * (size_t)i + 1])) continue;
+                const double x = params.rect_x + lat_x[i % LW] * params.step;
+                const double y = params.rect_y + lat_y[i / LW] * params.step;
+                rp.push_back({x, y});
+                dp.push_back({x + anchor_uv[2 * (size_t)i], y + anchor_uv[2 * (size_t)i + 1]});
+            }
+            double Hr[9];
+            if (rp.size() >= 8 && semper_geom::fit_homography(rp, dp, 6.0, Hr)) {
+                std::copy(Hr, Hr + 9, learned_H);
+                std::copy(Hr, Hr + 9, E.last_learned_.H);
+                setup_model();
+            }
+            E.last_learned_.ms += (float)ms_since(t_g);
+            E.last_learned_.anchor_uv = anchor_uv;
+            guided = true;
+        }
 
         auto solve_lattice = [&](bool sim) -> float {
             quality = Quality::NONE;
@@ -1044,6 +1161,12 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 float gs[6] = {globalU, globalV, 0, 0, 0, 0};
                 if (sim && !model_at(t.cx, t.cy, gs)) {
                     gs[0] = globalU; gs[1] = globalV; gs[2] = gs[3] = gs[4] = gs[5] = 0;
+                }
+                // the learned seeding's own guess for this anchor under its model
+                if (sim && guided && std::isfinite(anchor_uv[2 * (size_t)i]) &&
+                    std::isfinite(anchor_uv[2 * (size_t)i + 1])) {
+                    gs[0] = anchor_uv[2 * (size_t)i];
+                    gs[1] = anchor_uv[2 * (size_t)i + 1];
                 }
                 for (int k = 0; k < 6; ++k) t.g[k] = gs[k];
                 tk.push_back(t);
@@ -1171,6 +1294,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                 // anchors' statistics counted for that seeding only
                 st_anchor = HostStats();
                 model_H = nullptr;
+                guided = false;
                 plain_estimate();
                 setup_model();
                 seed_lattice();

@@ -117,6 +117,9 @@ struct LearnedSeed {
     int pairs = 0, inliers = 0, anchors = 0;
     float err_mean = 0.0f, err_max = 0.0f;
     float ms = 0.0f;  // device time of the network's stages
+    // the network's displacement guess per anchor-lattice node (row-major,
+    // 2 floats each, NaN where none) under the proposed model
+    std::vector<float> anchor_uv;
 };
 
 // The raw result of one patch-subset solve (match_anchor's solve).

@@ -161,7 +161,7 @@ void ProposalNet::predict_warped(const uint8_t* d_ref, const uint8_t* d_def, int
     if (W < 2 || H < 2 || pitch < W || f < 1 || f > 16) throw std::invalid_argument("proposal: frame or factor");
     centres_.ensure(std::max(centres_.n, (size_t)K * 8));
     check(cudaMemcpyAsync(centres_.p, maps, (size_t)K * 32, cudaMemcpyHostToDevice, st), "H2D maps");
-    check(dic::pp_cut_warped(d_ref, d_def, W, H, pitch, centres_.p, K, f, w_.act[0], st), "cut warped");
+    check(dic::pp_cut_warped(d_ref, d_def, W, H, pitch, centres_.p, K, f, w_.act[0], w_.y, st), "cut warped");
     check(dic::pp_forward(params_.p, w_, K, st), "proposal forward");
     check(cudaMemcpyAsync(out, w_.out, (size_t)K * 6 * 4, cudaMemcpyDeviceToHost, st), "D2H out");
     check(cudaStreamSynchronize(st), "sync");

@@ -488,6 +488,15 @@ SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_propos
     return 0;
 }
 
+SEMPER_C_API int semper_b200_learned_guesses(semper_engine* eng, float* uv, int32_t capacity) {
+    if (eng == nullptr || capacity < 0 || (uv == nullptr && capacity > 0)) return SEMPER_ERR_INIT;
+    const std::vector<float>& g = eng->engine.last_learned().anchor_uv;
+    const int32_t n = (int32_t)(g.size() / 2);
+    if (capacity < 2 * n) return n;
+    std::copy(g.begin(), g.end(), uv);
+    return n;
+}
+
 SEMPER_C_API int semper_b200_last_learned(semper_engine* eng, double out[18]) {
     if (eng == nullptr || out == nullptr) return SEMPER_ERR_INIT;
     const semper_b200::LearnedSeed& L = eng->engine.last_learned();

@@ -101,10 +101,11 @@ __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const 
 // K is walked 16 at a time through shared memory (pairs of bf16 packed in a
 // word, rows padded to 9 words so the fragment reads meet distinct banks).
 // Blocks along z take `kchunk`-long slices of K; with `atomic` they add into
-// C (zeroed first), else they store.
+// C (zeroed first), else they store, block z at C + z * slice (slice 0: all
+// into C), so that split partials can be summed later in a fixed order.
 template <class LA, class LB>
 __global__ void __launch_bounds__(128) gemm_kernel(LA A, LB Bt, int M, int N, int K, float* C, int ldc, int kchunk,
-                                                   int atomic) {
+                                                   int atomic, size_t slice) {
     __shared__ uint32_t As[64][9];
     __shared__ uint32_t Bs[64][9];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(128) gemm_kernel(LA A, LB Bt, int M, int N, in
                 for (int q = 0; q < 2; ++q) {
                     const int c = c0 + q;
                     if (c >= N) continue;
-                    float* dst = C + (size_t)r * ldc + c;
+                    float* dst = C + (size_t)blockIdx.z * slice + (size_t)r * ldc + c;
                     if (atomic)
                         atomicAdd(dst, acc[mt][nt][2 * h + q]);
                     else
@@ -189,17 +190,41 @@ cudaError_t gemm(LA A, LB Bt, int M, int N, int K, float* C, int ldc, int splits
     kchunk = (kchunk + 15) & ~15;
     splits = (K + kchunk - 1) / kchunk;
     const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64), (unsigned)splits);
-    gemm_kernel<<<grid, 128, 0, st>>>(A, Bt, M, N, K, C, ldc, kchunk, splits > 1 ? 1 : 0);
+    gemm_kernel<<<grid, 128, 0, st>>>(A, Bt, M, N, K, C, ldc, kchunk, splits > 1 ? 1 : 0, (size_t)0);
     return cudaGetLastError();
 }
 
+// The forward's GEMMs: K split over enough blocks to fill the GPU when M is
+// small (at least 64 of K per split, and no more partial slices than the
+// scratch `cap` floats hold), each split storing its own M x N slice of C;
+// `used` returns the slice count for the reduction that follows.
+template <class LA, class LB>
+cudaError_t gemm_sliced(LA A, LB Bt, int M, int N, int K, float* C, size_t cap, int& used, cudaStream_t st) {
+    used = 1;
+    if (M <= 0 || N <= 0 || K <= 0) return cudaSuccess;
+    const int blocks = ((N + 63) / 64) * ((M + 63) / 64);
+    int splits = (2 * 148 + blocks - 1) / blocks;
+    splits = min(splits, max(1, K / 64));
+    splits = (int)min((size_t)splits, max((size_t)1, cap / ((size_t)M * N)));
+    splits = max(1, splits);
+    int kchunk = (K + splits - 1) / splits;
+    kchunk = (kchunk + 15) & ~15;
+    splits = (K + kchunk - 1) / kchunk;
+    used = splits;
+    const dim3 grid((unsigned)((N + 63) / 64), (unsigned)((M + 63) / 64), (unsigned)splits);
+    gemm_kernel<<<grid, 128, 0, st>>>(A, Bt, M, N, K, C, N, kchunk, 0, (size_t)M * N);
+    return cudaGetLastError();
+}
 
-// y[M x C] + bias -> bf16 activation (ReLU) or, with out32, FP32 output.
+// y[M x C] (the sum of `slices` partial M x C slices, in slice order) +
+// bias -> bf16 activation (ReLU) or, with out32, FP32 output.
 __global__ void bias_act_kernel(const float* __restrict__ y, const float* __restrict__ bias, int M, int C,
-                                uint16_t* act, float* out32) {
+                                uint16_t* act, float* out32, int slices) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= (size_t)M * C) return;
-    const float v = __fadd_rn(y[i], bias[i % C]);
+    float t = y[i];
+    for (int z = 1; z < slices; ++z) t = __fadd_rn(t, y[(size_t)z * M * C + i]);
+    const float v = __fadd_rn(t, bias[i % C]);
     if (out32)
         out32[i] = v;
     else
@@ -456,31 +481,35 @@ __device__ __forceinline__ float bilinear_u8(const uint8_t* im, int W, int H, in
     return (1.0f - fy) * ((1.0f - fx) * r0[0] + fx * r0[1]) + fy * ((1.0f - fx) * r1[0] + fx * r1[1]);
 }
 
+// Pair blockIdx.x's patch pixels blockIdx.y * 256 + threadIdx.x, before
+// normalisation, into v32 [B][2][4096].
 __global__ void __launch_bounds__(256) cut_warped_kernel(const uint8_t* __restrict__ ref,
                                                          const uint8_t* __restrict__ def, int W, int H, int pitch,
-                                                         const float* __restrict__ maps, int f, uint16_t* x) {
-    extern __shared__ float vbuf[];
-    float(*v)[4096] = reinterpret_cast<float(*)[4096]>(vbuf);
+                                                         const float* __restrict__ maps, int f, float* v32) {
     const int k = blockIdx.x;
     const float* m = maps + 8 * k;
     const int ax = (int)m[0], ay = (int)m[1];
     const float inv_f2 = 1.0f / (float)(f * f);
-    for (int i = threadIdx.x; i < 4096; i += 256) {
-        const int u = i & 63, w = i >> 6;
-        float r = 0.0f, d = 0.0f;
-        for (int sj = 0; sj < f; ++sj)
-            for (int si = 0; si < f; ++si) {
-                const int X = ax + f * (u - 32) + si, Y = ay + f * (w - 32) + sj;
-                r += px_clamped(ref, W, H, pitch, X, Y);
-                const float xd = m[2] * (float)X + m[3] * (float)Y + m[6];
-                const float yd = m[4] * (float)X + m[5] * (float)Y + m[7];
-                d += bilinear_u8(def, W, H, pitch, xd, yd);
-            }
-        v[0][i] = r * inv_f2;
-        v[1][i] = d * inv_f2;
-    }
-    __syncthreads();
-    normalise_store(v, x + (size_t)k * 8192);
+    const int i = blockIdx.y * 256 + threadIdx.x;
+    const int u = i & 63, w = i >> 6;
+    float r = 0.0f, d = 0.0f;
+    for (int sj = 0; sj < f; ++sj)
+        for (int si = 0; si < f; ++si) {
+            const int X = ax + f * (u - 32) + si, Y = ay + f * (w - 32) + sj;
+            r += px_clamped(ref, W, H, pitch, X, Y);
+            const float xd = m[2] * (float)X + m[3] * (float)Y + m[6];
+            const float yd = m[4] * (float)X + m[5] * (float)Y + m[7];
+            d += bilinear_u8(def, W, H, pitch, xd, yd);
+        }
+    v32[(size_t)k * 8192 + i] = r * inv_f2;
+    v32[(size_t)k * 8192 + 4096 + i] = d * inv_f2;
+}
+
+// One block per pair: its two channels of v32 normalised into x.
+__global__ void __launch_bounds__(256) normalise_kernel(const float* __restrict__ v32, uint16_t* x) {
+    const int k = blockIdx.x;
+    normalise_store(reinterpret_cast<float(*)[4096]>(const_cast<float*>(v32 + (size_t)k * 8192)),
+                    x + (size_t)k * 8192);
 }
 
 inline unsigned nblocks(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
@@ -534,20 +563,24 @@ void pp_work_carve(PpWork& w, void* base, int B) {
 cudaError_t pp_forward(const float* params, PpWork& w, int B, cudaStream_t st) {
     if (B <= 0 || B > w.max_batch) return cudaErrorInvalidValue;
     const PpLayout L = pp_layout();
+    const size_t cap = kScratchElems * (size_t)w.max_batch;
     cudaError_t e;
+    int sl = 1;
     for (int l = 0; l < 5; ++l) {
         const int Hs = kPpSide >> l, Ci = kPpChannels[l], Co = kPpChannels[l + 1];
         const int M = B * (Hs / 2) * (Hs / 2), K = 9 * Ci;
-        e = gemm(LdIm2Col<false>{w.act[l], Hs, Hs, Ci}, LdF32Row{params + L.w[l], K}, M, Co, K, w.y, Co, 1, st);
+        e = gemm_sliced(LdIm2Col<false>{w.act[l], Hs, Hs, Ci}, LdF32Row{params + L.w[l], K}, M, Co, K, w.y, cap, sl,
+                        st);
         if (e != cudaSuccess) return e;
-        bias_act_kernel<<<nblocks((size_t)M * Co), 256, 0, st>>>(w.y, params + L.b[l], M, Co, w.act[l + 1], nullptr);
+        bias_act_kernel<<<nblocks((size_t)M * Co), 256, 0, st>>>(w.y, params + L.b[l], M, Co, w.act[l + 1], nullptr,
+                                                                 sl);
     }
-    e = gemm(LdBfRow{w.act[5], kPpFc0}, LdF32Row{params + L.w[5], kPpFc0}, B, kPpFc1, kPpFc0, w.y, kPpFc1, 1, st);
+    e = gemm_sliced(LdBfRow{w.act[5], kPpFc0}, LdF32Row{params + L.w[5], kPpFc0}, B, kPpFc1, kPpFc0, w.y, cap, sl, st);
     if (e != cudaSuccess) return e;
-    bias_act_kernel<<<nblocks((size_t)B * kPpFc1), 256, 0, st>>>(w.y, params + L.b[5], B, kPpFc1, w.h, nullptr);
-    e = gemm(LdBfRow{w.h, kPpFc1}, LdF32Row{params + L.w[6], kPpFc1}, B, kPpOut, kPpFc1, w.y, kPpOut, 1, st);
+    bias_act_kernel<<<nblocks((size_t)B * kPpFc1), 256, 0, st>>>(w.y, params + L.b[5], B, kPpFc1, w.h, nullptr, sl);
+    e = gemm_sliced(LdBfRow{w.h, kPpFc1}, LdF32Row{params + L.w[6], kPpFc1}, B, kPpOut, kPpFc1, w.y, cap, sl, st);
     if (e != cudaSuccess) return e;
-    bias_act_kernel<<<nblocks((size_t)B * kPpOut), 256, 0, st>>>(w.y, params + L.b[6], B, kPpOut, nullptr, w.out);
+    bias_act_kernel<<<nblocks((size_t)B * kPpOut), 256, 0, st>>>(w.y, params + L.b[6], B, kPpOut, nullptr, w.out, sl);
     return cudaGetLastError();
 }
 
@@ -622,12 +655,10 @@ cudaError_t pp_cut_pairs(const uint8_t* ref, const uint8_t* def, int W, int H, i
 }
 
 cudaError_t pp_cut_warped(const uint8_t* ref, const uint8_t* def, int W, int H, int pitch, const float* maps, int B,
-                          int f, uint16_t* x, cudaStream_t st) {
+                          int f, uint16_t* x, float* scratch, cudaStream_t st) {
     if (B <= 0) return cudaSuccess;
-    cudaError_t e =
-        cudaFuncSetAttribute(cut_warped_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * 4096 * 4);
-    if (e != cudaSuccess) return e;
-    cut_warped_kernel<<<B, 256, 2 * 4096 * 4, st>>>(ref, def, W, H, pitch, maps, f, x);
+    cut_warped_kernel<<<dim3((unsigned)B, 16), 256, 0, st>>>(ref, def, W, H, pitch, maps, f, scratch);
+    normalise_kernel<<<B, 256, 0, st>>>(scratch, x);
     return cudaGetLastError();
 }
 

@@ -66,9 +66,10 @@ cudaError_t pp_cut_pairs(const uint8_t* ref, const uint8_t* def, int W, int H, i
 // second patch takes, for each sample X of its first patch (the f x f pixels
 // around centre (ax_k, ay_k)), `def` at x' = A_k X + b_k (bilinear, clamped
 // to the frame); maps [B][8] = ax, ay, a00, a01, a10, a11, bx, by. With the
-// map the true one, the two patches show the same material.
+// map the true one, the two patches show the same material. scratch: B x 8192
+// floats for the values before normalisation.
 cudaError_t pp_cut_warped(const uint8_t* ref, const uint8_t* def, int W, int H, int pitch, const float* maps, int B,
-                          int f, uint16_t* x, cudaStream_t st);
+                          int f, uint16_t* x, float* scratch, cudaStream_t st);
 
 // Synthetic training pairs from a float speckle image S (W x H): pair k gets
 // a random centre c, rotation, small stretch and shear and translation t; its

@@ -47,7 +47,7 @@ EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b20
                "semper_b200_proposal_set_params", "semper_b200_proposal_get_params", "semper_b200_proposal_forward",
                "semper_b200_proposal_gradients", "semper_b200_proposal_synth", "semper_b200_proposal_train",
                "semper_b200_proposal_predict_warped",
-               "semper_b200_set_proposal", "semper_b200_last_learned"]
+               "semper_b200_set_proposal", "semper_b200_last_learned", "semper_b200_learned_guesses"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -130,6 +130,7 @@ def lib():
         L.semper_b200_proposal_predict_warped.argtypes = [_vp, _u8p, _u8p, ctypes.c_int32, ctypes.c_int32, _f32p,
                                                           ctypes.c_int32, ctypes.c_int32, _f32p]
         L.semper_b200_set_proposal.argtypes = [_vp, _vp, ctypes.c_int]
+        L.semper_b200_learned_guesses.argtypes = [_vp, _f32p, ctypes.c_int32]
         L.semper_b200_last_learned.argtypes = [_vp, _f64p]
         L.semper_b200_set_tma_wait_limit.argtypes = [_vp, ctypes.c_int]
         L.semper_b200_last_tma_timeout.argtypes = [_vp]
@@ -277,6 +278,15 @@ class Engine:
                 "inliers": int(o[4]), "anchors": int(o[5]), "err_mean_px": float(o[6]), "err_max_px": float(o[7]),
                 "ms": float(o[8]), "H": o[9:18].reshape(3, 3).copy()}
 
+    def learned_guesses(self) -> np.ndarray:
+        """[n][2] displacement guesses per anchor-lattice node of the last
+        learned seeding (NaN where none; empty when it did not run)."""
+        n = lib().semper_b200_learned_guesses(self._h, None, 0)
+        out = np.zeros((max(n, 0), 2), np.float32)
+        if n > 0:
+            lib().semper_b200_learned_guesses(self._h, _p(out, _f32p), 2 * n)
+        return out
+
     def set_tma_wait_limit(self, polls: int) -> int:
         return lib().semper_b200_set_tma_wait_limit(self._h, polls)
 
@@ -294,6 +304,10 @@ class Engine:
                 "peaks": (o[7], o[8]), "H": o[9:].reshape(3, 3).copy()}
 
 
+# The proposal network's trained weights (train_proposal.py), shipped with the package.
+PROPOSAL_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "proposal.npy")
+
+
 class Proposal:
     """The learned seed proposal network (semper_b200_proposal_*): two 64x64
     patches -> the affine map between them, on BF16 tensor-core kernels."""
@@ -303,6 +317,13 @@ class Proposal:
         if not self._h:
             raise RuntimeError("semper_b200_proposal_create failed")
         self.max_batch = max_batch
+
+    @classmethod
+    def trained(cls, max_batch: int = 256, path: str | None = None) -> "Proposal":
+        """A network with the shipped trained weights (or those at `path`)."""
+        net = cls(max_batch)
+        net.set_params(np.load(path or PROPOSAL_WEIGHTS))
+        return net
 
     def close(self):
         h = getattr(self, "_h", None)
