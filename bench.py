@@ -56,6 +56,11 @@ WORKLOADS = {
                    "smooth random field of 5 px amplitude (Gaussian covariance, length 300 px), noise sigma 2; "
                    "step 8, subset 41, strain window 41, 4x4 bicubic; rect the centred 2744x2744 square that "
                    "stays inside the deformed frame at any rotation; fixed reference (frames 2+)"),
+    "cfg4-learned": ("large deformation, learned seeding: the cfg4-large pair (4096x4096, rotation ~U[0,180) deg, "
+                     "translation up to 60 px, 5 px random field, noise sigma 2; step 8, subset 41, strain window "
+                     "41, 4x4 bicubic, the centred 2744x2744 rect) seeded by the proposal network with its shipped "
+                     "weights (global model and per-anchor guesses, judged by the lattice's keep rule); fixed "
+                     "reference (frames 2+)"),
 }
 WORKLOAD = WORKLOADS["cfg1"]
 
@@ -190,6 +195,33 @@ def accuracy_sample(eng, ref, dfm, prm, warp, p, gm):
             "vs_true_field_rms_px": float(np.sqrt(np.mean(t ** 2))), "vs_true_field_max_px": float(t.max())}
 
 
+def compare_seedings(ref, dfm, prm, warp):
+    """The same pair seeded three ways, one run each after a warm-up run, out
+    of the timed region: the proposal network, the device global-motion
+    estimate, and the anchor lattice alone (the reference's AUTO_SEARCH
+    without a model). Points, seeding time and error against the true field."""
+    import semper_b200 as sb
+
+    res = {}
+    for mode in ("learned", "global_motion", "lattice_only"):
+        eng = sb.Engine()
+        eng.set_reference(ref)
+        if mode == "learned":
+            eng.set_proposal(sb.Proposal.trained(), True)
+        if mode != "global_motion":
+            eng.set_global_motion(False)
+        eng.run(dfm, prm)
+        rc, pts, _ = eng.run(dfm, prm)
+        t, _ = eng.last_timings()
+        r = {"points": int(rc), "seed_ms": round(t["seed"], 3), "total_ms": round(t["total"], 3)}
+        if rc > 0:
+            u, v = sb.displacement(warp, pts[:, 0], pts[:, 1])
+            r["vs_true_field_rms_px"] = float(np.sqrt(np.mean((pts[:, 2] - u) ** 2 + (pts[:, 3] - v) ** 2)))
+        res[mode] = r
+        eng.close()
+    return res
+
+
 REF_SAMPLE_SIDE = 1024
 
 
@@ -262,7 +294,7 @@ def measure_frames(args, wl, rank, world, local_rank, dist):
 
     import semper_b200 as sb
 
-    if wl == "cfg4-large":
+    if wl in ("cfg4-large", "cfg4-learned"):
         ref, dfm, prm, warp, _sim = sb.large_motion_pair(args.size, pair=rank)
     else:
         ref, dfm, prm, warp = sb.config_pair(4 if wl == "cfg4-plain" else 1, size=args.size, pair=rank)
@@ -272,6 +304,10 @@ def measure_frames(args, wl, rank, world, local_rank, dist):
 
     eng = sb.Engine()
     assert eng.set_reference(ref) == 0
+    net = None
+    if wl == "cfg4-learned":
+        net = sb.Proposal.trained()
+        assert eng.set_proposal(net, True) == 0
     d_def = torch.from_numpy(dfm).cuda()
     d_out = torch.empty(capacity, dtype=torch.float32, device="cuda")
 
@@ -338,6 +374,15 @@ def measure_frames(args, wl, rank, world, local_rank, dist):
     bpp = NCU_BYTES_PER_PIXEL_ITER.get(prm.subset_size) if not six else None
     traffic = None if bpp is None else bpp * a_pix
     gm = eng.last_global_motion()
+    learned = None
+    if net is not None:
+        L = eng.last_learned()
+        learned = {"kept": L["kept"], "network_ms": round(L["ms"], 3), "patch_pairs": L["pairs"],
+                   "grid_inliers": L["inliers"], "anchors_judging": L["anchors"],
+                   "model_vs_anchors_px": {"mean": round(L["err_mean_px"], 3), "max": round(L["err_max_px"], 3)}}
+        if L["kept"]:
+            gm = {"locked": True, "theta": float(np.arctan2(L["H"][1, 0], L["H"][0, 0])), "scale": 1.0,
+                  "t": (float(L["H"][0, 2]), float(L["H"][1, 2])), "H": L["H"]}
 
     out = {
         "value": value, "ms_per_step": ms_max,
@@ -372,6 +417,11 @@ def measure_frames(args, wl, rank, world, local_rank, dist):
         "clocks": clk.summary(),
         "gpu_launches": int(sum(c["launches"] for c in counts)),
     }
+    if learned is not None:
+        out["learned_seeding"] = learned
+        out.pop("global_model")
+        if rank == 0:
+            out["seeding_compared"] = compare_seedings(ref, dfm, prm, warp)
     if rank == 0 and world == 1 and not args.no_cpu:
         crc, cdt, catt, cpts, cp = cpu_sample(ref, dfm, prm, model=gm["H"] if gm["locked"] else None)
         out["cpu_baseline"] = {"value": crc / cdt, "unit": "points/s", "cores": len(os.sched_getaffinity(0)),
@@ -561,10 +611,10 @@ def main():
                     help="cfg1 only: skip the nested target-settings measurement (step 8, subset 41)")
     ap.add_argument("--size", type=int, default=4096,
                     help="image edge (default 4096, the benchmark workload; smaller sizes are for profiling)")
-    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg4-plain", "cfg4-large", "cfg3"],
+    ap.add_argument("--workload", default="cfg1", choices=["cfg1", "cfg2", "cfg4-plain", "cfg4-large", "cfg4-learned", "cfg3"],
                     help="cfg1 (the headline line), cfg2 (batched uneven pairs), cfg4-plain (the target "
-                         "settings), cfg4-large (large deformation seeded by the global-motion estimate), cfg3 "
-                         "(incremental sample)")
+                         "settings), cfg4-large (large deformation seeded by the global-motion estimate), "
+                         "cfg4-learned (the same pair seeded by the proposal network), cfg3 (incremental sample)")
     ap.add_argument("--pairs", type=int, default=256, help="cfg2: pairs per batch")
     ap.add_argument("--workers", type=int, default=8, help="cfg2: concurrent engines")
     ap.add_argument("--interval", type=int, default=1, help="cfg3: the session's update_interval")
