@@ -12,8 +12,8 @@
 //
 // The global-motion model (the reference's AKAZE homography, OpenCV) is an
 // input here: none, or a 3x3 homography supplied by the caller. The planar
-// geometry that the reference takes from OpenCV comes from the library's own
-// header (geometry.hpp), as the device pipeline uses it.
+// geometry that the reference takes from OpenCV is the oracle's own (geom.hpp),
+// under the rules the build fixed for it.
 #pragma once
 #include <chrono>
 #include <cstdint>
@@ -21,7 +21,7 @@
 #include <queue>
 #include <vector>
 
-#include "../../semper-dic-engine_b200/csrc/host/geometry.hpp"
+#include "geom.hpp"
 #include "solver.hpp"
 #include "strain.hpp"
 
@@ -346,14 +346,14 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
     Stats st_anchor, st_a, st_b;
     SolveInfo seeds;
     std::vector<Anchor> anchors;
-    std::vector<semper_geom::Pt> ref_pts, def_pts;
+    std::vector<oracle_geom::Pt> ref_pts, def_pts;
     float globalU = 0, globalV = 0;
     bool have_model = model_H != nullptr, model_full = false, model_rejected = false;
     double t_u = 0, t_v = 0;
     const double gcx = params.rect_x + 0.5 * params.rect_w, gcy = params.rect_y + 0.5 * params.rect_h;
     auto model_at = [&](double x, double y, float g6[6]) {
         double X, Y, J[4];
-        if (!semper_geom::homography_at(model_H, x, y, X, Y, J)) return false;
+        if (!oracle_geom::homography_at(model_H, x, y, X, Y, J)) return false;
         g6[0] = (float)(X - x); g6[1] = (float)(Y - y);
         g6[2] = (float)(J[0] - 1.0); g6[3] = (float)J[1];
         g6[4] = (float)J[2]; g6[5] = (float)(J[3] - 1.0);
@@ -463,7 +463,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
             globalU = median_of(us);
             globalV = median_of(vs);
             const float roi_area = (float)(params.rect_w * params.rect_h);
-            seeds.coverage = roi_area > 0.f ? (float)semper_geom::hull_area(ref_pts) / roi_area : 0.f;
+            seeds.coverage = roi_area > 0.f ? (float)oracle_geom::hull_area(ref_pts) / roi_area : 0.f;
         }
         const float frac = seeds.attempted > 0 ? (float)seeds.accepted / (float)seeds.attempted : 0.f;
         if (seeds.accepted >= kAnchorFullMinVertices && frac >= kAnchorFullFraction &&
@@ -489,7 +489,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
         bool refitted = false;
         if (seeds.accepted >= kAnchorRefitMinPoints) {
             double Hf[9];
-            if (semper_geom::fit_homography(ref_pts, def_pts, kAnchorRefitRansacPx, Hf)) {
+            if (oracle_geom::fit_homography(ref_pts, def_pts, kAnchorRefitRansacPx, Hf)) {
                 homography.assign(Hf, Hf + 9);
                 refitted = true;
             }
@@ -522,20 +522,20 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
     const size_t NG = (size_t)gridW * gridH;
     std::vector<float> gu(NG, globalU), gv(NG, globalV), gux(NG, 0.f), guy(NG, 0.f), gvx(NG, 0.f), gvy(NG, 0.f);
     std::vector<unsigned char> in_mesh(NG, 0);
-    struct ATri { semper_geom::Pt p[3]; int64_t X[3], Y[3]; double u, v, ux, uy, vx, vy; float bx, by, bw, bh; };
+    struct ATri { oracle_geom::Pt p[3]; int64_t X[3], Y[3]; double u, v, ux, uy, vx, vy; float bx, by, bw, bh; };
     std::vector<ATri> tris;
     {
-        std::vector<semper_geom::Pt> ins;
+        std::vector<oracle_geom::Pt> ins;
         std::vector<int> ins_of;
         for (size_t i = 0; i < ref_pts.size(); ++i)
             if (ref_pts[i].x > 0 && ref_pts[i].x < W && ref_pts[i].y > 0 && ref_pts[i].y < H) {
                 ins.push_back(ref_pts[i]);
                 ins_of.push_back((int)i);
             }
-        for (const semper_geom::Tri& t : semper_geom::delaunay(ins)) {
+        for (const oracle_geom::Tri& t : oracle_geom::delaunay(ins)) {
             ATri at;
             const int vi[3] = {t.a, t.b, t.c};
-            semper_geom::Pt dst[3];
+            oracle_geom::Pt dst[3];
             for (int k = 0; k < 3; ++k) {
                 at.p[k] = ins[vi[k]];
                 dst[k] = def_pts[ins_of[vi[k]]];
@@ -543,7 +543,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
                 at.Y[k] = std::llround(at.p[k].y);
             }
             double M[6];
-            if (!semper_geom::affine3(at.p, dst, M)) continue;
+            if (!oracle_geom::affine3(at.p, dst, M)) continue;
             const double detF = M[0] * M[4] - M[1] * M[3];
             if (!std::isfinite(detF) || std::fabs(detF) <= 1e-3) continue;
             at.ux = M[0] - 1.0; at.uy = M[1]; at.vx = M[3]; at.vy = M[4] - 1.0; at.u = M[2]; at.v = M[5];
@@ -569,7 +569,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
             const size_t idx = (size_t)y * gridW + x;
             for (const ATri& t : tris) {
                 if (px < t.bx || px > t.bx + t.bw || py < t.by || py > t.by + t.bh) continue;
-                if (semper_geom::tri_contains(t.X, t.Y, (int64_t)px, (int64_t)py)) {
+                if (oracle_geom::in_triangle(t.X, t.Y, (int64_t)px, (int64_t)py)) {
                     assign(idx, t, px, py, kMeshInTriangle);
                     break;
                 }
@@ -587,7 +587,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
                 for (size_t ti = 0; ti < tris.size(); ++ti) {
                     const ATri& t = tris[ti];
                     if (px < t.bx + LIM || px > t.bx + t.bw - LIM || py < t.by + LIM || py > t.by + t.bh - LIM) continue;
-                    const double d = semper_geom::tri_signed_distance(t.p, {px, py});
+                    const double d = oracle_geom::signed_distance(t.p, {px, py});
                     if (d >= LIM && (float)d > best) { best = (float)d; bi = (int)ti; }
                 }
                 if (bi >= 0) assign(idx, tris[bi], px, py, kMeshExtrapolated);
@@ -600,7 +600,7 @@ int run_full_field(RefCache<T>& cache, const uint8_t* def_gray, const uint8_t* m
                 if (in_mesh[idx] || grid[idx].solved) continue;
                 const double px = params.rect_x + (double)x * params.step, py = params.rect_y + (double)y * params.step;
                 double X, Y, J[4];
-                if (!semper_geom::homography_at(homography.data(), px, py, X, Y, J)) continue;
+                if (!oracle_geom::homography_at(homography.data(), px, py, X, Y, J)) continue;
                 gu[idx] = (float)(X - px); gv[idx] = (float)(Y - py);
                 gux[idx] = (float)(J[0] - 1.0); guy[idx] = (float)J[1];
                 gvx[idx] = (float)J[2]; gvy[idx] = (float)(J[3] - 1.0);
