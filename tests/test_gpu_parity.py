@@ -379,3 +379,19 @@ def test_tma_wait_that_runs_out_falls_back_bit_exact():
     assert e.set_tma_wait_limit(0) == 0
     rc2, pts2, _ = e.run(dfm, prm)
     assert e.last_tma_timeout() == 0 and np.array_equal(pts2, pts0)
+
+
+def test_path_c_seed_bit_exact():
+    """Path C seeds the field: the anchor lattice's nodes are all masked
+    (tests/scenarios.py), so the routing finds no seed and the central
+    search's first converging candidate starts the Path B flood. The device
+    field equals the CPU restatement's, bit for bit, with the metrics showing
+    no anchor, no Path A point and every point from Path B."""
+    import scenarios
+
+    ref, dfm, mask, prm = scenarios.lattice_masked_pair()
+    d, o = _run_both(ref, dfm, prm, mask=mask)
+    met = d[2]
+    assert d[0] > 2000
+    assert met[16] == 0 and met[19] == 0 and met[3] == 0 and met[4] > 3000
+    _assert_field_equal(d, o)

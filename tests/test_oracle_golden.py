@@ -236,3 +236,25 @@ def test_full_field_golden_at_task_bounds(oracle_lib, golden_dir, scenario):
         assert rc == f["codes"][scenario]
         out.append(pts)
     ff_task_bound_check(out[0], out[1], f[f"points{scenario}"], scenario)
+
+
+def test_path_c_seeds_a_lattice_masked_pair(oracle_lib):
+    """The restatement's Path C on a pair whose anchor lattice is masked out
+    (tests/scenarios.py), with no global model: only a converged central seed
+    (full_field_path_c.cpp:27-156) lets the solve return points (without one
+    an unlocked solve returns -5). Every point then comes from the Path B
+    flood, and it recovers the pair's known translation and stretch."""
+    import scenarios
+
+    ref, dfm, mask, prm = scenarios.lattice_masked_pair()
+    o = oracle_lib.Oracle(False)
+    assert o.set_reference(ref, mask) == 0
+    p = [prm.rect_x, prm.rect_y, prm.rect_w, prm.rect_h, prm.step, prm.subset_size, prm.strain_window, 0]
+    rc, pts, met = o.run(dfm, p, mask=mask)
+    assert rc > 2000
+    assert met[16] == 0 and met[19] == 0 and met[21] == 0  # no lattice quality, no anchor, no model
+    assert met[3] == 0 and met[4] == met[1] + met[20] + met[23]  # every point from Path B
+    pts = pts.reshape(-1, 8)
+    x, y = pts[:, 0], pts[:, 1]
+    assert np.abs(pts[:, 2] - (2.3 + 0.002 * x)).max() < 0.05
+    assert np.abs(pts[:, 3] - (-1.7 - 0.001 * y)).max() < 0.05
