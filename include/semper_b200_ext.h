@@ -116,6 +116,41 @@ SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jo
    none; valid until the next call on the runner. */
 SEMPER_C_API const char* semper_b200_batch_last_error(semper_b200_batch* b);
 
+/* Batched incremental sequences (no counterpart in the reference; each
+   sequence is solved exactly as its own semper_incremental handle would solve
+   it, src/pipeline/incremental_session.cpp:120-549). The runner holds
+   `sequences` sessions, each with its own engine and stream on the current
+   device. One process call advances every listed sequence by one frame, the
+   sequences concurrently (a host thread each), so their kernels and copies
+   interleave on the device and one sequence's host steps overlap the others'
+   solves. */
+typedef struct semper_b200_inc_batch semper_b200_inc_batch;
+
+typedef struct semper_b200_inc_frame {
+    int32_t sequence;          /* which session, 0 <= sequence < sequences */
+    const uint8_t* frame;      /* width*height bytes, raw 8-bit gray, the sequence's size */
+    float* out;                /* out_capacity floats: packed points, as semper_incremental_process */
+    int32_t out_capacity;
+    float* metrics;            /* metrics_len floats, or NULL */
+    int32_t metrics_len;
+    semper_incremental_info info; /* written */
+    int32_t result;            /* written: semper_incremental_process's return value for this frame */
+} semper_b200_inc_frame;
+
+/* NULL on failure or for sequences <= 0. */
+SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create(int32_t sequences);
+SEMPER_C_API void semper_b200_inc_batch_destroy(semper_b200_inc_batch* b);
+/* semper_incremental_init of one sequence on raw 8-bit frames of width x
+   height (mask: the same size, or NULL). Same return codes. */
+SEMPER_C_API int semper_b200_inc_batch_init(semper_b200_inc_batch* b, int32_t sequence, const uint8_t* reference,
+                                            const uint8_t* mask, int32_t width, int32_t height,
+                                            const semper_params* params, int32_t update_interval);
+/* One frame for each entry; entries must name distinct sequences. Returns 0
+   when every entry has run (each entry's own code is in its `result`), or -3
+   for a NULL or busy runner, a sequence out of range or named twice. Frame
+   and output buffers must stay valid until it returns. */
+SEMPER_C_API int semper_b200_inc_batch_process(semper_b200_inc_batch* b, semper_b200_inc_frame* frames, int32_t n);
+
 /* The learned seed proposal network (no counterpart in the reference): two
    64x64 patches in, the 6-parameter affine map between them out; BF16
    tensor-core kernels with FP32 accumulation for inference and training.

@@ -47,7 +47,9 @@ EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b20
                "semper_b200_proposal_set_params", "semper_b200_proposal_get_params", "semper_b200_proposal_forward",
                "semper_b200_proposal_gradients", "semper_b200_proposal_synth", "semper_b200_proposal_train",
                "semper_b200_proposal_predict_warped",
-               "semper_b200_set_proposal", "semper_b200_last_learned", "semper_b200_learned_guesses"]
+               "semper_b200_set_proposal", "semper_b200_last_learned", "semper_b200_learned_guesses",
+               "semper_b200_inc_batch_create", "semper_b200_inc_batch_destroy", "semper_b200_inc_batch_init",
+               "semper_b200_inc_batch_process"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -66,6 +68,10 @@ class IncrementalInfo(ctypes.Structure):
                 ("taylor_fallbacks", ctypes.c_int32), ("lost_this_frame", ctypes.c_int32)]
 
 
+class IncFrame(ctypes.Structure):
+    """semper_b200_inc_frame (include/semper_b200_ext.h)."""
+
+
 class BatchJob(ctypes.Structure):
     """semper_b200_job (include/semper_b200_ext.h)."""
     _fields_ = [("reference", ctypes.c_void_p), ("deformed", ctypes.c_void_p), ("mask", ctypes.c_void_p),
@@ -73,6 +79,10 @@ class BatchJob(ctypes.Structure):
                 ("out", ctypes.c_void_p), ("out_capacity", ctypes.c_int32), ("metrics", ctypes.c_void_p),
                 ("metrics_len", ctypes.c_int32), ("result", ctypes.c_int32)]
 
+
+IncFrame._fields_ = [("sequence", ctypes.c_int32), ("frame", ctypes.c_void_p), ("out", ctypes.c_void_p),
+                     ("out_capacity", ctypes.c_int32), ("metrics", ctypes.c_void_p), ("metrics_len", ctypes.c_int32),
+                     ("info", IncrementalInfo), ("result", ctypes.c_int32)]
 
 PROGRESS_CB = ctypes.CFUNCTYPE(None, ctypes.c_int, ctypes.c_void_p)
 
@@ -139,6 +149,12 @@ def lib():
         L.semper_b200_batch_destroy.argtypes = [_vp]
         L.semper_b200_batch_run.argtypes = [_vp, ctypes.POINTER(BatchJob), ctypes.c_int32]
         L.semper_b200_incremental_profile.argtypes = [_vp, _f64p]
+        L.semper_b200_inc_batch_create.argtypes = [ctypes.c_int32]
+        L.semper_b200_inc_batch_create.restype = _vp
+        L.semper_b200_inc_batch_destroy.argtypes = [_vp]
+        L.semper_b200_inc_batch_init.argtypes = [_vp, ctypes.c_int32, _u8p, _u8p, ctypes.c_int32, ctypes.c_int32,
+                                                 ctypes.POINTER(SemperParams), ctypes.c_int32]
+        L.semper_b200_inc_batch_process.argtypes = [_vp, ctypes.POINTER(IncFrame), ctypes.c_int32]
         L.semper_b200_batch_last_error.argtypes = [_vp]
         L.semper_b200_batch_last_error.restype = ctypes.c_char_p
         L.semper_b200_last_global_motion.argtypes = [_vp, _f64p]
@@ -527,6 +543,59 @@ class Incremental:
         keys = ["total", "run", "match", "warp_mask", "adopt", "pack", "matches", "runs",
                 "prep", "pool", "seed", "mesh", "path_a", "path_b", "strain", "solve_total"]
         return dict(zip(keys, map(float, o)))
+
+
+class IncrementalBatch:
+    """semper_b200_inc_batch: several frame sequences advanced together, one
+    session each, their solves interleaved on the device."""
+
+    def __init__(self, sequences: int):
+        self._h = lib().semper_b200_inc_batch_create(sequences)
+        if not self._h:
+            raise RuntimeError("semper_b200_inc_batch_create failed")
+        self.sequences = sequences
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        self._h = None
+        if h and _lib is not None:  # at interpreter exit the library may be gone already
+            _lib.semper_b200_inc_batch_destroy(h)
+
+    __del__ = close
+
+    def init(self, seq: int, ref, prm: SemperParams, update_interval: int, mask=None) -> int:
+        g = np.ascontiguousarray(ref, np.uint8)
+        m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
+        return lib().semper_b200_inc_batch_init(self._h, seq, _p(g, _u8p), _p(m, _u8p), g.shape[1], g.shape[0],
+                                                ctypes.byref(prm), update_interval)
+
+    def process(self, frames: dict, capacity: int, metrics_len: int = 24):
+        """frames: {sequence: frame}. Returns {sequence: (rc, points, metrics, info)}."""
+        seqs = sorted(frames)
+        arr = (IncFrame * len(seqs))()
+        keep = []
+        for i, q in enumerate(seqs):
+            d = np.ascontiguousarray(frames[q], np.uint8)
+            out = np.zeros(max(capacity, 1), np.float32)
+            met = np.zeros(max(metrics_len, 1), np.float32)
+            keep.append((d, out, met))
+            arr[i].sequence = q
+            arr[i].frame = d.ctypes.data
+            arr[i].out = out.ctypes.data
+            arr[i].out_capacity = capacity
+            arr[i].metrics = met.ctypes.data
+            arr[i].metrics_len = metrics_len
+        rc = lib().semper_b200_inc_batch_process(self._h, arr, len(seqs))
+        if rc != 0:
+            raise RuntimeError(f"semper_b200_inc_batch_process returned {rc}")
+        res = {}
+        for i, q in enumerate(seqs):
+            r = arr[i].result
+            _, out, met = keep[i]
+            info = IncrementalInfo()
+            ctypes.memmove(ctypes.byref(info), ctypes.byref(arr[i].info), ctypes.sizeof(IncrementalInfo))
+            res[q] = (r, out[: max(r, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info)
+        return res
 
 
 def version() -> str:

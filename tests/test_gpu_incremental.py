@@ -166,3 +166,36 @@ def test_coasting_and_anchor_matches_match_restatement(interval):
     print(f"interval {interval}: {matches} anchor matches, {taylor} Taylor samples")
     assert taylor > 0
     assert matches > 0
+
+
+def test_batched_sequences_match_restatement():
+    """Three sequences (own seeds, update intervals and one with a mask)
+    advanced together by semper_b200_inc_batch_process, their solves
+    interleaved on the device: every frame of every sequence equals the CPU
+    restatement's session on that sequence alone, bit for bit."""
+    prm = ((16, 16, 224, 224), 8, 21, 21)
+    yy, xx = np.mgrid[0:256, 0:256]
+    mask = np.full((256, 256), 255, np.uint8)
+    mask[(xx - 120) ** 2 + (yy - 140) ** 2 < 25 ** 2] = 0
+    setups = [(31, 1, None), (17, 3, mask), (53, 0, None)]
+    seqs = [sequence(seed=s, frames=5) for s, _, _ in setups]
+    cap = (256 // 8) ** 2 * 8
+    b = sb.IncrementalBatch(len(setups))
+    oras = []
+    for q, ((seed, interval, m), (ref, _)) in enumerate(zip(setups, seqs)):
+        assert b.init(q, ref, sb.params(*prm), interval, mask=m) == 0
+        o = oracle.IncrementalOracle()
+        assert o.init(ref, [*prm[0], prm[1], prm[2], prm[3], 0], interval, mask=m) == 0
+        oras.append(o)
+    for t in range(5):
+        got = b.process({q: seqs[q][1][t] for q in range(len(setups))}, cap)
+        for q in range(len(setups)):
+            assert_same(got[q], oras[q].process(seqs[q][1][t], cap))
+            assert got[q][0] > 300
+    # a sequence named twice, or out of range, is refused
+    arr = (sb.IncFrame * 2)()
+    arr[0].sequence = arr[1].sequence = 0
+    assert sb.lib().semper_b200_inc_batch_process(b._h, arr, 2) == sb.SEMPER_ERR_INIT
+    arr[1].sequence = 7
+    assert sb.lib().semper_b200_inc_batch_process(b._h, arr, 2) == sb.SEMPER_ERR_INIT
+    b.close()

@@ -383,15 +383,28 @@ def test_tma_wait_that_runs_out_falls_back_bit_exact():
 
 def test_path_c_seed_bit_exact():
     """Path C seeds the field: the anchor lattice's nodes are all masked
-    (tests/scenarios.py), so the routing finds no seed and the central
-    search's first converging candidate starts the Path B flood. The device
-    field equals the CPU restatement's, bit for bit, with the metrics showing
-    no anchor, no Path A point and every point from Path B."""
+    (tests/scenarios.py) and the global-motion front end is off (the
+    reference without an AKAZE model), so the routing finds no seed and the
+    central search's first converging candidate starts the Path B flood. The
+    device field equals the CPU restatement's, bit for bit, with the metrics
+    showing no anchor, no Path A point and every point from Path B. With the
+    front end on (its default) the model's guess field feeds Path A instead,
+    and the two still agree."""
     import scenarios
 
     ref, dfm, mask, prm = scenarios.lattice_masked_pair()
-    d, o = _run_both(ref, dfm, prm, mask=mask)
+    e = sb.Engine()
+    assert e.set_global_motion(False) == 0
+    assert e.set_reference(ref, mask) == 0
+    d = e.run(dfm, prm, mask=mask)
+    o = oracle.Oracle(False)
+    o.set_reference(ref, mask)
+    p = [prm.rect_x, prm.rect_y, prm.rect_w, prm.rect_h, prm.step, prm.subset_size, prm.strain_window, 0]
+    ores = o.run(dfm, p, mask=mask)
     met = d[2]
     assert d[0] > 2000
-    assert met[16] == 0 and met[19] == 0 and met[3] == 0 and met[4] > 3000
-    _assert_field_equal(d, o)
+    assert met[16] == 0 and met[19] == 0 and met[21] == 0 and met[3] == 0 and met[4] > 3000
+    _assert_field_equal(d, ores)
+    d2, o2 = _run_both(ref, dfm, prm, mask=mask)
+    assert d2[0] > 2000
+    _assert_field_equal(d2, o2)
