@@ -468,7 +468,7 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
-def run_cfg3(args, rank):
+def run_cfg3(args, rank, world=1, local_rank=0):
     """cfg3 (batched incremental DIC): args.sequences 2048x2048 sequences, each
     with its own seed, under a monotone uniaxial stretch (25 % over 128
     frames) plus a rigid rotation (30 deg over 128 frames), noise sigma 1.5,
@@ -478,125 +478,184 @@ def run_cfg3(args, rank):
     one frame of every sequence; warm-up frames are solved but not timed.
     Frames 1..W+K of the 128-frame sequences are run (the first W+K of the
     workload's frames)."""
-    if rank != 0:
-        return 0
     import math
 
     import torch
 
     import semper_b200 as sb
 
+    dist = _init_dist(world, local_rank)
     n = args.size if args.size != 4096 else 2048
-    S = max(1, args.sequences)
+    S_all = max(1, args.sequences)
+    # N > 1: the sequences are split over the ranks (equal cost each), every
+    # rank advancing its own on its GPU; no data crosses ranks
+    seq_ids = sb.shard([1] * S_all, rank, world)
+    S = len(seq_ids)
     total = args.warmup + args.steps
     t_gen = time.perf_counter()
-    refs = [sb.speckle(n, n, 3000 + 17 * q) for q in range(S)]
+    refs = [sb.speckle(n, n, 3000 + 17 * q) for q in seq_ids]
 
     def frame(q, t):
         th, s = math.radians(30.0) * t / 128.0, 0.25 * t / 128.0
         a = (math.cos(th) * (1 + s) - 1, -math.sin(th), math.sin(th) * (1 + s), math.cos(th) - 1)
         return sb.speckle(n, n, 3000 + 17 * q, sb.warp_block(cx=n / 2, cy=n / 2, a=a), 1.5, 4000 + 1000 * q + t)
 
-    frames = [[frame(q, t) for q in range(S)] for t in range(1, total + 1)]
+    frames = [[frame(q, t) for q in seq_ids] for t in range(1, total + 1)]
     gen_s = time.perf_counter() - t_gen
     m = n // 8
     prm = sb.params((m, m, n - 2 * m, n - 2 * m), 6, 21, 21)
     cap = ((n - 2 * m) // 6) ** 2 * 8
-    b = sb.IncrementalBatch(S)
+    b = sb.IncrementalBatch(max(S, 1))
     for q in range(S):
         assert b.init(q, refs[q], prm, args.interval) == 0
-    ms, pts, updates, all_pts, all_ms = [], [], 0, 0, 0.0
-    with ClockSampler(0) as clk:
-        for i, fr in enumerate(frames):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            res = b.process({q: fr[q] for q in range(S)}, cap)
-            dt = time.perf_counter() - t0
-            got = [res[q][0] for q in range(S)]
-            assert min(got) > 0, got
-            all_pts += sum(got)
-            all_ms += 1000 * dt
-            if i >= args.warmup:
-                ms.append(1000 * dt)
-                pts.append(sum(got))
-                updates += sum(res[q][3].reference_updated for q in range(S))
+    acc = {"i": 0, "all_pts": 0}
+
+    def step():
+        fr = frames[acc["i"]]
+        acc["i"] += 1
+        res = b.process({q: fr[q] for q in range(S)}, cap)
+        got = [res[q][0] for q in range(S)]
+        assert not got or min(got) > 0, got
+        acc["all_pts"] += sum(got)
+        return sum(got), sum(res[q][3].reference_updated for q in range(S))
+
+    t_w = time.perf_counter()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    warm_ms = 1000 * (time.perf_counter() - t_w)
+    with ClockSampler(local_rank) as clk:
+        ms_rank, outs = _timed_region(dist, step, args.steps)
     b.close()
-    mean_ms = statistics.mean(ms)
-    value = sum(pts) / (sum(ms) / 1000.0)
+    pts_rank = sum(o[0] for o in outs)
+    value, mean_ms = aggregate(pts_rank, ms_rank / args.steps, args.steps, dist, "cuda")
+    sums = torch.tensor([pts_rank / args.steps, sum(o[1] for o in outs), acc["all_pts"]], device="cuda",
+                        dtype=torch.float64)
+    all_ms_t = torch.tensor([warm_ms + ms_rank], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(sums)
+        dist.all_reduce(all_ms_t, op=dist.ReduceOp.MAX)
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    pts_step, updates, all_pts = (float(x) for x in sums.tolist())
+    all_ms = float(all_ms_t.item())
+    S = S_all
     line = {
-        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": 1,
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"cfg3: {S} sequences of {n}x{n} speckle (own seeds), stretch 25 % + rotation 30 deg "
                                f"over 128 frames, noise 1.5, subset 21, step 6, window 21, update_interval "
                                f"{args.interval}; a step advances every sequence by one frame "
                                f"(semper_b200_inc_batch_process); frames {args.warmup + 1}..{total} timed after "
                                f"{args.warmup} warm-up frames",
-                   "sequences": S, "frames_timed_per_sequence": len(ms), "reference_updates": updates,
-                   "points_per_step": statistics.mean(pts), "frame_generation_s": round(gen_s, 1),
-                   "l2": "inputs larger than L2: each step reads 8 new 4 MiB frames and every session's planes"},
+                   "sequences": S, "frames_timed_per_sequence": args.steps, "reference_updates": int(updates),
+                   "parallelism": f"the sequences split over {world} GPU(s)",
+                   "points_per_step": pts_step, "frame_generation_s": round(gen_s, 1),
+                   "l2": f"inputs larger than L2: each step reads {S} new {n * n >> 20} MiB frames and every "
+                         f"session's planes"},
         "frames_per_s": S * 1000.0 / mean_ms,
-        "from_frame1": {"frames": S * total, "points": all_pts, "ms": round(all_ms, 3),
+        "from_frame1": {"frames": S * total, "points": int(all_pts), "ms": round(all_ms, 3),
                         "points_per_s": all_pts / (all_ms / 1000.0), "frames_per_s": S * total / (all_ms / 1000.0)},
         "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": S * n * n,
-                "d2h_bytes_per_step": int(statistics.mean(pts)) * 32},
+                "d2h_bytes_per_step": int(pts_step) * 32},
         "clocks": clk.summary(),
     }
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_cfg2(args, rank):
+def _init_dist(world, local_rank):
+    """NCCL process group for N > 1 (None at N = 1), with a short timeout."""
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def _timed_region(dist, fn, steps):
+    """Runs fn() `steps` times between a barrier and a device synchronize on
+    both sides; returns this rank's wall time in ms and fn's results."""
+    import torch
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = [fn() for _ in range(steps)]
+    torch.cuda.synchronize()
+    ms = 1000 * (time.perf_counter() - t0)
+    if dist:
+        dist.barrier()
+    return ms, out
+
+
+def run_cfg2(args, rank, world=1, local_rank=0):
     """cfg2 (batched uneven solves): args.pairs independent pairs of side
     U{256..2048} with their own affine warps, masks, subsets and steps,
     solved concurrently through semper_b200_batch_run (host frames in, host
     points out). A step is one batch of every pair; the time is the host wall
     time of the call with the device idle on both sides."""
-    if rank != 0:
-        return 0
     import torch
 
     import semper_b200 as sb
 
+    dist = _init_dist(world, local_rank)
     t0 = time.perf_counter()
-    jobs = sb.batch_jobs(args.pairs, seed=0)
+    # N > 1: the fixed batch is split over the ranks (sb.shard, by cost),
+    # each rank solving its share on its own GPU; no data crosses ranks
+    all_jobs = sb.batch_job_params(args.pairs, seed=0)
+    all_prm = [p for p, _ in all_jobs]
+    mine = sb.shard([sb.job_cost(p) for p in all_prm], rank, world)
+    jobs = sb.batch_jobs(args.pairs, seed=0, only=mine)
     gen_s = time.perf_counter() - t0
     b = sb.Batch(workers=args.workers)
     for _ in range(args.warmup):
         res = b.run(jobs)
-    ms, pts = [], []
-    with ClockSampler(0) as clk:
-        for _ in range(args.steps):
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            res = b.run(jobs)
-            torch.cuda.synchronize()
-            ms.append(1000 * (time.perf_counter() - t0))
-            pts.append(sum(max(r[0], 0) for r in res))
-    mean_ms = statistics.mean(ms)
-    value = sum(pts) / (sum(ms) / 1000.0)
-    nodes = sum((j["prm"].rect_w // j["prm"].step) * (j["prm"].rect_h // j["prm"].step) for j in jobs)
+    with ClockSampler(local_rank) as clk:
+        ms_rank, outs = _timed_region(dist, lambda: b.run(jobs), args.steps)
+    res = outs[-1]
+    pts_rank = sum(sum(max(r[0], 0) for r in o) for o in outs)
+    value, mean_ms = aggregate(pts_rank, ms_rank / args.steps, args.steps, dist, "cuda")
+    pts_t = torch.tensor([pts_rank / args.steps], device="cuda", dtype=torch.float64)
+    fail_t = torch.tensor([sum(1 for r in res if r[0] <= 0)], device="cuda", dtype=torch.float64)
+    if dist:
+        dist.all_reduce(pts_t)
+        dist.all_reduce(fail_t)
+    if dist:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    nodes = sum((p.rect_w // p.step) * (p.rect_h // p.step) for p in all_prm)
     line = {
-        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "weak",
+        "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": mean_ms, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"cfg2: {args.pairs} independent pairs, side U{{256..2048}}, affine warps (|rot| <= 10 "
                                f"deg, stretch <= 3 %, shift <= 8 px), 1-3 circular mask holes removing U[0, 40 %], "
                                f"subset U{{15,21,31,41}}, step U{{4,8}}, window = subset; {args.workers} concurrent "
-                               f"engines",
-                   "grid_nodes": nodes, "points_per_step": statistics.mean(pts),
-                   "jobs_failed": sum(1 for r in res if r[0] <= 0), "generation_s": round(gen_s, 1),
+                               f"engines per GPU",
+                   "parallelism": f"the batch split over {world} GPU(s) by cost (semper_b200.shard)",
+                   "grid_nodes": nodes, "points_per_step": float(pts_t.item()),
+                   "jobs_failed": int(fail_t.item()), "generation_s": round(gen_s, 1),
                    "timing": "host wall time of semper_b200_batch_run (frames from host memory, points to host "
                              "memory), device synchronised on both sides; value and e2e are the same measurement",
                    "l2": "inputs larger than L2: every pair's planes and pool are rebuilt per step"},
         "frames_per_s": args.pairs * 1000.0 / mean_ms,
         "e2e": {"value": value, "unit": "points/s",
-                "h2d_bytes_per_step": int(sum(2 * j["ref"].size + (0 if j["mask"] is None else 2 * j["mask"].size)
-                                              for j in jobs)),
-                "d2h_bytes_per_step": int(statistics.mean(pts) * 32)},
+                "h2d_bytes_per_step": int(sum(2 * p.rect_w * p.rect_h * (2 if m else 1) for p, m in all_jobs)),
+                "d2h_bytes_per_step": int(pts_t.item() * 32)},
         "clocks": clk.summary(),
     }
-    if not args.no_cpu:
+    if not args.no_cpu and world == 1:
         sys.path.insert(0, os.path.join(REPO, "oracle"))
         import oracle
 
@@ -645,9 +704,9 @@ def main():
     if args.impl == "reference":
         return run_reference(args, rank)
     if args.workload == "cfg3":
-        return run_cfg3(args, rank)
+        return run_cfg3(args, rank, world, local_rank)
     if args.workload == "cfg2":
-        return run_cfg2(args, rank)
+        return run_cfg2(args, rank, world, local_rank)
     return run_b200(args, rank, world, local_rank)
 
 

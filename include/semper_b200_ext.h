@@ -85,7 +85,8 @@ SEMPER_C_API int semper_b200_set_global_motion(semper_engine* eng, int on);
 SEMPER_C_API int semper_b200_last_global_motion(semper_engine* eng, double out[18]);
 
 /* Batched solves: many independent pairs, each with its own size, mask and
-   settings, solved concurrently on the current device. No counterpart in the
+   settings, solved concurrently on the current device (or several GPUs,
+   semper_b200_batch_create_on). No counterpart in the
    reference (its callers loop over semper_set_reference + semper_run); each
    job's result, metrics and return code are exactly those of that loop on a
    fresh handle. */
@@ -107,6 +108,12 @@ typedef struct semper_b200_batch semper_b200_batch;
 /* A batch runner with `workers` engines (<= 0: 8), each with its own stream
    and host thread, on the current device. NULL on failure. */
 SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers);
+/* The same with the engines spread over `n_devices` GPUs: engine i on
+   devices[i % n_devices], so a batch's jobs spread over the GPUs as the
+   workers take them (each job solved on one GPU, with the results a lone
+   engine gives it). n_devices 0: the current device. NULL on failure. */
+SEMPER_C_API semper_b200_batch* semper_b200_batch_create_on(int32_t workers, const int32_t* devices,
+                                                             int32_t n_devices);
 SEMPER_C_API void semper_b200_batch_destroy(semper_b200_batch* b);
 /* Solves every job (largest first, spread over the workers) and returns 0
    when all have run (each job's own code is in its `result`), or -3 for a
@@ -119,11 +126,10 @@ SEMPER_C_API const char* semper_b200_batch_last_error(semper_b200_batch* b);
 /* Batched incremental sequences (no counterpart in the reference; each
    sequence is solved exactly as its own semper_incremental handle would solve
    it, src/pipeline/incremental_session.cpp:120-549). The runner holds
-   `sequences` sessions, each with its own engine and stream on the current
-   device. One process call advances every listed sequence by one frame, the
-   sequences concurrently (a host thread each), so their kernels and copies
-   interleave on the device and one sequence's host steps overlap the others'
-   solves. */
+   `sequences` sessions, each with its own engine and stream. One process
+   call advances every listed sequence by one frame, the sequences
+   concurrently (a host thread each), so their kernels and copies interleave
+   on the device and one sequence's host steps overlap the others' solves. */
 typedef struct semper_b200_inc_batch semper_b200_inc_batch;
 
 typedef struct semper_b200_inc_frame {
@@ -139,6 +145,10 @@ typedef struct semper_b200_inc_frame {
 
 /* NULL on failure or for sequences <= 0. */
 SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create(int32_t sequences);
+/* The same with sequence q's session on devices[q % n_devices] (n_devices 0:
+   the current device). */
+SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create_on(int32_t sequences, const int32_t* devices,
+                                                                     int32_t n_devices);
 SEMPER_C_API void semper_b200_inc_batch_destroy(semper_b200_inc_batch* b);
 /* semper_incremental_init of one sequence on raw 8-bit frames of width x
    height (mask: the same size, or NULL). Same return codes. */

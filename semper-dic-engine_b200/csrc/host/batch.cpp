@@ -3,6 +3,8 @@
 //
 // Each worker owns an Engine (its own stream, device buffers and staging) and
 // a host thread; jobs are taken largest first from a shared counter. The
+// engines may sit on several GPUs (semper_b200_batch_create_on): jobs then
+// spread over the devices as the workers take them. The
 // engines' persistent solve kernels, image passes and copies then overlap on
 // the device, and one job's host-side steps (lattice routing, Delaunay,
 // Path B claims) run while the others' kernels execute. Every job is solved
@@ -16,6 +18,7 @@
 #include <memory>
 #include <mutex>
 #include <numeric>
+#include <stdexcept>
 #include <string>
 #include <thread>
 #include <vector>
@@ -29,7 +32,8 @@ using semper_b200::Engine;
 using semper_b200::Params;
 
 struct semper_b200_batch {
-    int device = 0;
+    int device = 0;                 // the caller's device at creation
+    std::vector<int> dev_of;        // each engine's device
     std::vector<std::unique_ptr<Engine>> engines;
     std::atomic<bool> busy{false};
     std::mutex err_mu;
@@ -66,22 +70,45 @@ int run_job(Engine& e, semper_b200_job& j) {
 
 extern "C" {
 
-SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers) {
+SEMPER_C_API semper_b200_batch* semper_b200_batch_create_on(int32_t workers, const int32_t* devices,
+                                                             int32_t n_devices) {
+    if (n_devices < 0 || (n_devices > 0 && devices == nullptr)) return nullptr;
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return nullptr;
+    std::unique_ptr<semper_b200_batch> b(new semper_b200_batch());
+    b->device = cur;
     try {
         if (workers <= 0) workers = 8;
-        auto* b = new semper_b200_batch();
-        if (cudaGetDevice(&b->device) != cudaSuccess) {
-            delete b;
-            return nullptr;
+        for (int i = 0; i < workers; ++i) {
+            const int dev = n_devices > 0 ? devices[i % n_devices] : cur;
+            if (cudaSetDevice(dev) != cudaSuccess) throw std::runtime_error("device");
+            b->engines.emplace_back(new Engine());  // its stream and buffers on `dev`
+            b->dev_of.push_back(dev);
         }
-        for (int i = 0; i < workers; ++i) b->engines.emplace_back(new Engine());
-        return b;
     } catch (...) {
+        semper_b200_batch_destroy(b.release());
+        cudaSetDevice(cur);
         return nullptr;
     }
+    cudaSetDevice(cur);
+    return b.release();
 }
 
-SEMPER_C_API void semper_b200_batch_destroy(semper_b200_batch* b) { delete b; }
+SEMPER_C_API semper_b200_batch* semper_b200_batch_create(int32_t workers) {
+    return semper_b200_batch_create_on(workers, nullptr, 0);
+}
+
+SEMPER_C_API void semper_b200_batch_destroy(semper_b200_batch* b) {
+    if (b == nullptr) return;
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    for (size_t i = 0; i < b->engines.size(); ++i) {
+        if (i < b->dev_of.size()) cudaSetDevice(b->dev_of[i]);
+        b->engines[i].reset();  // freed with its own device current
+    }
+    if (have) cudaSetDevice(cur);
+    delete b;
+}
 
 SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jobs, int32_t n_jobs) {
     if (b == nullptr || (jobs == nullptr && n_jobs > 0) || n_jobs < 0) return SEMPER_ERR_INIT;
@@ -99,8 +126,9 @@ SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jo
         b->last_error.clear();
     }
     std::atomic<int> next{0};
-    auto work = [&](Engine& e) {
-        cudaSetDevice(b->device);
+    auto work = [&](size_t w) {
+        Engine& e = *b->engines[w];
+        cudaSetDevice(b->dev_of[w]);
         for (;;) {
             const int k = next.fetch_add(1);
             if (k >= n_jobs) break;
@@ -123,9 +151,12 @@ SEMPER_C_API int semper_b200_batch_run(semper_b200_batch* b, semper_b200_job* jo
     };
     const size_t nw = std::min(b->engines.size(), (size_t)std::max(n_jobs, 1));
     std::vector<std::thread> threads;
-    for (size_t w = 1; w < nw; ++w) threads.emplace_back(work, std::ref(*b->engines[w]));
-    work(*b->engines[0]);
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    for (size_t w = 1; w < nw; ++w) threads.emplace_back(work, w);
+    work(0);
     for (auto& t : threads) t.join();
+    if (have) cudaSetDevice(cur);
     b->busy.store(false, std::memory_order_release);
     return 0;
 }

@@ -1,10 +1,11 @@
 // Batched incremental sequences: several frame sequences, each tracked by its
-// own incremental session (one engine, one stream, its own device state), on
-// one GPU. A process call advances every listed sequence by one frame, each on
+// own incremental session (one engine, one stream, its own device state). A
+// process call advances every listed sequence by one frame, each on
 // its own host thread, so the sessions' kernels and copies interleave on the
 // device while one session's host steps (anchor matches, update schedule,
 // packing) overlap the others' solves. A sequence is solved exactly as a lone
-// semper_incremental handle solves it: the sessions share nothing.
+// semper_incremental handle solves it: the sessions share nothing. The
+// sessions may sit on several GPUs (semper_b200_inc_batch_create_on).
 #include <atomic>
 #include <cstdint>
 #include <memory>
@@ -19,13 +20,20 @@ struct semper_b200_inc_batch {
     int device = 0;
     struct Seq {
         semper_incremental* h = nullptr;
+        int device = 0;  // the session's device
         int width = 0, height = 0;
     };
     std::vector<Seq> seqs;
     std::atomic<bool> busy{false};
     ~semper_b200_inc_batch() {
+        int cur = 0;
+        const bool have = cudaGetDevice(&cur) == cudaSuccess;
         for (Seq& s : seqs)
-            if (s.h) semper_incremental_destroy(s.h);
+            if (s.h) {
+                cudaSetDevice(s.device);
+                semper_incremental_destroy(s.h);
+            }
+        if (have) cudaSetDevice(cur);
     }
 };
 
@@ -44,20 +52,34 @@ struct BusyGuard {
 
 extern "C" {
 
-SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create(int32_t sequences) {
-    if (sequences <= 0) return nullptr;
+SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create_on(int32_t sequences, const int32_t* devices,
+                                                                     int32_t n_devices) {
+    if (sequences <= 0 || n_devices < 0 || (n_devices > 0 && devices == nullptr)) return nullptr;
+    int cur = 0;
+    if (cudaGetDevice(&cur) != cudaSuccess) return nullptr;
+    semper_b200_inc_batch* out = nullptr;
     try {
         std::unique_ptr<semper_b200_inc_batch> b(new semper_b200_inc_batch());
-        if (cudaGetDevice(&b->device) != cudaSuccess) return nullptr;
+        b->device = cur;
         b->seqs.resize((size_t)sequences);
-        for (auto& s : b->seqs) {
-            s.h = semper_incremental_create();
-            if (!s.h) return nullptr;
+        bool ok = true;
+        for (size_t q = 0; q < b->seqs.size() && ok; ++q) {
+            auto& s = b->seqs[q];
+            s.device = n_devices > 0 ? devices[q % (size_t)n_devices] : cur;
+            ok = cudaSetDevice(s.device) == cudaSuccess;
+            if (ok) s.h = semper_incremental_create();  // its engine and stream on s.device
+            ok = ok && s.h != nullptr;
         }
-        return b.release();
+        if (ok) out = b.release();
     } catch (...) {
-        return nullptr;
+        out = nullptr;
     }
+    cudaSetDevice(cur);
+    return out;
+}
+
+SEMPER_C_API semper_b200_inc_batch* semper_b200_inc_batch_create(int32_t sequences) {
+    return semper_b200_inc_batch_create_on(sequences, nullptr, 0);
 }
 
 SEMPER_C_API void semper_b200_inc_batch_destroy(semper_b200_inc_batch* b) { delete b; }
@@ -71,8 +93,12 @@ SEMPER_C_API int semper_b200_inc_batch_init(semper_b200_inc_batch* b, int32_t se
     if (!g.owned) return SEMPER_ERR_INIT;
     auto& s = b->seqs[(size_t)sequence];
     const size_t len = (size_t)width * (size_t)height;
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
+    cudaSetDevice(s.device);
     const int rc = semper_incremental_init(s.h, reference, len, mask, mask ? len : 0, width, height, params,
                                            update_interval);
+    if (have) cudaSetDevice(cur);
     s.width = rc == 0 ? width : 0;
     s.height = rc == 0 ? height : 0;
     return rc;
@@ -88,9 +114,11 @@ SEMPER_C_API int semper_b200_inc_batch_process(semper_b200_inc_batch* b, semper_
         if (q < 0 || q >= (int32_t)b->seqs.size() || named[(size_t)q]) return SEMPER_ERR_INIT;
         named[(size_t)q] = 1;
     }
+    int cur = 0;
+    const bool have = cudaGetDevice(&cur) == cudaSuccess;
     auto one = [b](semper_b200_inc_frame& f) {
-        cudaSetDevice(b->device);
         auto& s = b->seqs[(size_t)f.sequence];
+        cudaSetDevice(s.device);
         f.info = semper_incremental_info{};
         if (s.width <= 0 || f.frame == nullptr) {
             f.result = SEMPER_ERR_INIT;
@@ -108,6 +136,7 @@ SEMPER_C_API int semper_b200_inc_batch_process(semper_b200_inc_batch* b, semper_
     }
     if (n > 0) one(frames[0]);
     for (auto& t : threads) t.join();
+    if (have) cudaSetDevice(cur);
     return 0;
 }
 

@@ -49,7 +49,7 @@ EXT_SYMBOLS = ["semper_b200_last_timings", "semper_b200_run_device", "semper_b20
                "semper_b200_proposal_predict_warped",
                "semper_b200_set_proposal", "semper_b200_last_learned", "semper_b200_learned_guesses",
                "semper_b200_inc_batch_create", "semper_b200_inc_batch_destroy", "semper_b200_inc_batch_init",
-               "semper_b200_inc_batch_process"]
+               "semper_b200_inc_batch_process", "semper_b200_batch_create_on", "semper_b200_inc_batch_create_on"]
 DIC_SYMBOLS = ["dic_cuda_image_prep", "dic_cuda_grid_scan", "dic_cuda_hessian_pool", "dic_cuda_solve",
                "dic_cuda_solve_scratch_bytes",
                "dic_cuda_median_pass", "dic_cuda_clear_failed", "dic_cuda_vsg", "dic_cuda_pack_scratch_bytes",
@@ -151,6 +151,10 @@ def lib():
         L.semper_b200_incremental_profile.argtypes = [_vp, _f64p]
         L.semper_b200_inc_batch_create.argtypes = [ctypes.c_int32]
         L.semper_b200_inc_batch_create.restype = _vp
+        L.semper_b200_inc_batch_create_on.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+        L.semper_b200_inc_batch_create_on.restype = _vp
+        L.semper_b200_batch_create_on.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_int32), ctypes.c_int32]
+        L.semper_b200_batch_create_on.restype = _vp
         L.semper_b200_inc_batch_destroy.argtypes = [_vp]
         L.semper_b200_inc_batch_init.argtypes = [_vp, ctypes.c_int32, _u8p, _u8p, ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.POINTER(SemperParams), ctypes.c_int32]
@@ -410,8 +414,13 @@ class Proposal:
 class Batch:
     """semper_b200_batch: independent pairs solved concurrently."""
 
-    def __init__(self, workers: int = 8):
-        self._h = lib().semper_b200_batch_create(workers)
+    def __init__(self, workers: int = 8, devices=None):
+        """devices: GPU ordinals the workers spread over (None: the current one)."""
+        if devices:
+            dv = (ctypes.c_int32 * len(devices))(*devices)
+            self._h = lib().semper_b200_batch_create_on(workers, dv, len(devices))
+        else:
+            self._h = lib().semper_b200_batch_create(workers)
         if not self._h:
             raise RuntimeError("semper_b200_batch_create failed")
 
@@ -460,15 +469,48 @@ class Batch:
         return res
 
 
-def batch_jobs(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int = 2048):
+def job_cost(prm) -> int:
+    """A job's relative solve cost for sharding: grid nodes x subset pixels."""
+    return (prm.rect_w // prm.step) * (prm.rect_h // prm.step) * prm.subset_size * prm.subset_size
+
+
+def shard(costs, rank: int, world: int) -> list:
+    """The indices of `costs` that rank `rank` of `world` takes: largest cost
+    first, each to the least-loaded rank (the lowest rank on a tie). Every
+    rank computes the same assignment, so the shards cover every index exactly
+    once with no exchange between ranks."""
+    if world <= 1:
+        return list(range(len(costs)))
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += costs[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def batch_job_params(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int = 2048):
+    """The params (and whether a mask comes with each) of batch_jobs(n, seed,
+    ...) without generating any frame: [(params, has_mask)]."""
+    return [(j["prm"], j["has_mask"]) for j in batch_jobs(n, seed, min_side, max_side, frames=False)]
+
+
+def batch_jobs(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int = 2048, only=None,
+               frames: bool = True):
     """The batched uneven workload: n independent pairs, side ~ U{min_side..
     max_side} (square frames of seeded speckle as cfg0), each under its own
     affine warp (|rotation| <= 10 deg, stretch <= 3 % per axis, translation
     <= 8 px, about the frame centre) with noise sigma 1, and its own random
     circular holes in the mask (1-3 discs removing a fraction ~ U[0, 0.4] of
     the frame); per pair subset ~ {15, 21, 31, 41}, step ~ {4, 8},
-    strain window = subset, the whole frame as ROI."""
+    strain window = subset, the whole frame as ROI. `only`: the job indices
+    to build (a shard; every job is drawn the same either way), in index
+    order; `frames` False skips the frames and masks (params only)."""
     rng = np.random.default_rng(9000 + seed)
+    keep = None if only is None else set(only)
     jobs = []
     for k in range(n):
         side = int(rng.integers(min_side, max_side + 1))
@@ -481,11 +523,14 @@ def batch_jobs(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int =
         frac = rng.uniform(0.0, 0.4)
         nd = int(rng.integers(1, 4))
         mask = None
+        build = frames and (keep is None or k in keep)
         if frac > 0.0:
-            mask = np.full((side, side), 255, np.uint8)
+            mask = np.full((side, side), 255, np.uint8) if build else None
             r = side * np.sqrt(frac / (nd * np.pi))
             for _ in range(nd):
                 cx_, cy_ = rng.uniform(0, side, 2)
+                if not build:
+                    continue
                 x0, x1 = max(int(cx_ - r), 0), min(int(cx_ + r) + 2, side)
                 y0, y1 = max(int(cy_ - r), 0), min(int(cy_ + r) + 2, side)
                 yy, xx = np.mgrid[y0:y1, x0:x1]
@@ -493,10 +538,15 @@ def batch_jobs(n: int = 256, seed: int = 0, min_side: int = 256, max_side: int =
                 sub[(xx - cx_) ** 2 + (yy - cy_) ** 2 < r * r] = 0
         subset = int(rng.choice([15, 21, 31, 41]))
         step = int(rng.choice([4, 8]))
+        prm = params((0, 0, side, side), step, subset, subset)
+        if not frames:
+            jobs.append({"prm": prm, "warp": warp, "index": k, "has_mask": frac > 0.0})
+            continue
+        if keep is not None and k not in keep:
+            continue
         ref = speckle(side, side, 10000 + 17 * seed + k)
         dfm = speckle(side, side, 10000 + 17 * seed + k, warp, 1.0, 20000 + k)
-        jobs.append({"ref": ref, "dfm": dfm, "mask": mask, "prm": params((0, 0, side, side), step, subset, subset),
-                     "warp": warp})
+        jobs.append({"ref": ref, "dfm": dfm, "mask": mask, "prm": prm, "warp": warp, "index": k})
     return jobs
 
 
@@ -549,8 +599,13 @@ class IncrementalBatch:
     """semper_b200_inc_batch: several frame sequences advanced together, one
     session each, their solves interleaved on the device."""
 
-    def __init__(self, sequences: int):
-        self._h = lib().semper_b200_inc_batch_create(sequences)
+    def __init__(self, sequences: int, devices=None):
+        """devices: GPU ordinals the sessions spread over (None: the current one)."""
+        if devices:
+            dv = (ctypes.c_int32 * len(devices))(*devices)
+            self._h = lib().semper_b200_inc_batch_create_on(sequences, dv, len(devices))
+        else:
+            self._h = lib().semper_b200_inc_batch_create(sequences)
         if not self._h:
             raise RuntimeError("semper_b200_inc_batch_create failed")
         self.sequences = sequences

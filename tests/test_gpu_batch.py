@@ -70,3 +70,20 @@ def test_many_workers_mixed_subsets():
 
 def test_empty_batch():
     assert sb.Batch(workers=2).run([]) == []
+
+
+def test_batch_on_a_device_list(jobs):
+    """Engines created over a device list (every GPU this machine has, each
+    listed twice): the jobs as lone runs give them, whichever GPU solves
+    them. With one GPU this runs the list's plumbing on device 0."""
+    import torch
+
+    devs = [d for d in range(torch.cuda.device_count()) for _ in range(2)]
+    b = sb.Batch(workers=4, devices=devs)
+    got = b.run(jobs)
+    assert b.last_error == ""
+    for j, (rc, pts, met) in zip(jobs, got):
+        lrc, lpts, _ = _lone(j)
+        assert rc == lrc and np.array_equal(pts, lpts)
+    assert torch.cuda.current_device() == 0
+    b.close()

@@ -199,3 +199,27 @@ def test_batched_sequences_match_restatement():
     arr[1].sequence = 7
     assert sb.lib().semper_b200_inc_batch_process(b._h, arr, 2) == sb.SEMPER_ERR_INIT
     b.close()
+
+
+def test_batched_sequences_on_a_device_list():
+    """Sessions created over a device list (every GPU, each listed twice):
+    each sequence as its lone session gives it."""
+    import torch
+
+    devs = [d for d in range(torch.cuda.device_count()) for _ in range(2)]
+    prm = ((16, 16, 224, 224), 8, 21, 21)
+    seqs = [sequence(seed=s, frames=3) for s in (31, 53)]
+    cap = (256 // 8) ** 2 * 8
+    b = sb.IncrementalBatch(2, devices=devs)
+    lone = []
+    for q, (ref, _) in enumerate(seqs):
+        assert b.init(q, ref, sb.params(*prm), 1) == 0
+        s = sb.Incremental()
+        assert s.init(ref, sb.params(*prm), 1) == 0
+        lone.append(s)
+    for t in range(3):
+        got = b.process({q: seqs[q][1][t] for q in range(2)}, cap)
+        for q in range(2):
+            rc, pts, _, _ = lone[q].process(seqs[q][1][t], cap)
+            assert got[q][0] == rc > 300 and np.array_equal(got[q][1], pts)
+    b.close()
