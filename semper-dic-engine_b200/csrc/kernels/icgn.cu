@@ -851,7 +851,10 @@ StagedLayout staged_layout(int n, int tw, int th, bool stage = true, bool coop =
     StagedLayout L;
     L.tile_w = tw;
     L.tile_h = th;
-    L.off_tile = 640;
+    // the block's header (barrier, wait record, step matrix; with coop the
+    // masked-iteration matrix too) ahead of the 128-byte aligned tile; 512
+    // bytes without coop lets subset 31's fast pass hold 19 warps per SM
+    L.off_tile = coop ? 640 : 512;
     int p = L.off_tile + ((tw * th * 4 + 127) & ~127);
     const int arr = (n * 4 + 15) & ~15;
     L.off_vals = p;
@@ -2102,13 +2105,16 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
 // DIMC > 0: the subset size, the tile box and the pixels per lane known at
 // compile time (the launch checks they match), so the per-pixel loop
 // bookkeeping folds away; 32-bit validity masks up to 32 pixels per lane.
+// Subset 41's tile and sampled values (18.7 KB a warp) leave room for 12
+// warps per SM, so its registers are capped for 12 (no spills), the others'
+// for 18.
 template <bool SIX, int DIMC, bool STAGE>
-__global__ void __launch_bounds__(32, 18) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
+__global__ void __launch_bounds__(32, (DIMC == 41 ? 12 : 18)) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                   const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
     using Mask = std::conditional_t<(DIMC > 0 && DIMC * DIMC <= 1024), uint32_t, uint64_t>;
     constexpr int kTw = DIMC > 0 ? ((DIMC + (SIX ? 5 : 3) + 2 + 7 + 3) & ~3) : 0;
-    constexpr int kTh = DIMC > 0 ? DIMC + (SIX ? 5 : 3) + 2 + 4 : 0;
+    constexpr int kTh = DIMC > 0 ? DIMC + (SIX ? 5 : 3) + 2 + 2 : 0;
     WarpSolver<SIX, Mask, STAGE> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
                  DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
@@ -2432,11 +2438,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 void tile_box(int dim, int six, int& tw, int& th) {
     // the subset's support plus one pixel of rounding slack each side, three
-    // columns of alignment slack, and a margin of two pixels for the warp to
-    // move in before the tile is staged again
+    // columns of alignment slack, and a margin for the warp to move in before
+    // the tile is staged again: two pixels each way across, one up and down
+    // (two rows fewer of shared memory: subset 41's fast pass holds 12 warps
+    // per SM instead of 11)
     const int need = dim + (six ? 5 : 3) + 2;
     tw = ((need + 3 + 4) + 3) & ~3;
-    th = need + 4;
+    th = need + 2;
     if (tw > 256 || th > 256) tw = th = 0;
 }
 
