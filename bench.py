@@ -83,11 +83,11 @@ def _peaks():
 # DRAM bytes per subset pixel-iteration of the IC-GN fast pass (the Path A
 # launch), from one `ncu --set full` capture per solve setting (summaries in
 # profiles/icgn_solve_cfg1.md and profiles/icgn_solve_cfg4.md): the cfg1 pair
-# at 2048x2048, step 4, subset 31 read 149.6 MB over 969,920,963
+# at 2048x2048, step 4, subset 31 read and wrote 145.3 MB over 969,920,963
 # pixel-iterations; the target-settings pair at 2048x2048, step 8, subset 41
-# read 99.5 MB over 408,104,775. Traffic grows with the pixel-iterations, so a
+# 95.5 MB over 408,104,775. Traffic grows with the pixel-iterations, so a
 # launch's traffic is this figure times the launch's own pixel-iterations.
-NCU_BYTES_PER_PIXEL_ITER = {31: 149.6e6 / 969920963, 41: 99.5e6 / 408104775}
+NCU_BYTES_PER_PIXEL_ITER = {31: 145.3e6 / 969920963, 41: 95.5e6 / 408104775}
 
 
 class ClockSampler:
