@@ -204,13 +204,17 @@ SEMPER_C_API int semper_b200_proposal_predict_warped(semper_b200_proposal* p, co
                                                      const uint8_t* def, int32_t w, int32_t h, const float* maps,
                                                      int32_t batch, int32_t f, float* out);
 
-/* Learned seeding on an engine handle: with a proposal network (NULL: none)
-   and learned != 0, a run with no model set proposes its global model from
-   the network's predictions on patch pairs of the reference and the
-   deformed frame; the anchor lattice keeps or rejects it by the reference's
-   keep rule (full_field_anchors.cpp:204-279), and a rejected proposal falls
-   back to the global-motion estimate. The network must stay alive while the
-   handle may use it. Returns 0, or -3 for a NULL or busy handle. */
+/* Learned seeding on an engine handle: with a proposal network (NULL: none),
+   a run with no model set proposes its global model from the network's
+   predictions on patch pairs of the reference and the deformed frame, and
+   the anchor lattice keeps or rejects it by the reference's keep rule
+   (full_field_anchors.cpp:204-279). learned 1: the proposal first, a rejected
+   proposal falling back to the global-motion estimate; learned 2 (rescue):
+   the global-motion estimate first, the proposal only when the estimate does
+   not lock (and the plain lattice falls short of full quality) or the lattice
+   rejects its model, and a rejected proposal leaving the run as the estimate
+   seeded it; 0: off. The network must stay alive while the handle may use
+   it. Returns 0, or -3 for a NULL or busy handle or another mode. */
 SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_proposal* p, int learned);
 
 /* The last run's learned seeding: out[0] 1 when it ran, [1] a model was

@@ -589,8 +589,24 @@ struct Engine::Impl {
         a.cancel = E.d_cancel_;
         a.queue = solve_q.p;
         a.ref_no_ghost = ref_ghost ? 0 : 1;
+        a.tile_spread = tile_spread;
         (void)six;
         return a;
+    }
+
+    // The solves' TMA tiles follow the seeding model: a rotated or stretched
+    // subset's bounding box outgrows the subset by max(|J00| + |J01|,
+    // |J10| + |J11|) (J the model's local linear map at the ROI centre), and
+    // the tiles grow with it, 4 % beyond for the field's own variation.
+    // Below 1.03 the tiles of an unrotated subset serve.
+    float tile_spread = 0.f;
+    void set_tile_spread(const double* H, const Params& p) {
+        tile_spread = 0.f;
+        if (!H) return;
+        double X, Y, J[4];
+        if (!semper_geom::homography_at(H, p.rect_x + 0.5 * p.rect_w, p.rect_y + 0.5 * p.rect_h, X, Y, J)) return;
+        const double g = std::max(std::fabs(J[0]) + std::fabs(J[1]), std::fabs(J[2]) + std::fabs(J[3]));
+        if (std::isfinite(g) && g > 1.03) tile_spread = (float)std::min(1.04 * g, 4.0);
     }
 
     int solve_grid(int ntasks) {
@@ -1038,9 +1054,18 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         // ---------------------------------------------------------------- global model
         const auto t_seed = clk::now();
         E.last_learned_ = LearnedSeed{};
+        // the tiles follow this run's model only (solves outside a run, such
+        // as an incremental session's anchor matches, take the unrotated box)
+        tile_spread = 0.f;
+        struct SpreadReset {
+            float& v;
+            ~SpreadReset() { v = 0.f; }
+        } spread_reset{tile_spread};
         double learned_H[9];
-        const bool learned = !model_H && ref_gray && E.learned_ && E.proposal_ &&
-                             learned_model(params, d_def, learned_H);
+        // the caller's model, if any, rules out both front ends
+        const bool caller_model = model_H != nullptr;
+        bool learned = !caller_model && ref_gray && E.learned_ && !E.learned_rescue_ && E.proposal_ &&
+                       learned_model(params, d_def, learned_H);
         if (learned) model_H = learned_H;
         auto plain_estimate = [&]() {
             if (!model_H && E.global_motion_ && ref_gray) {
@@ -1098,6 +1123,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         locked = have_model;
         homography.clear();
         if (have_model) homography.assign(model_H, model_H + 9);
+        set_tile_spread(have_model ? model_H : nullptr, params);
         };
         setup_model();
 
@@ -1112,7 +1138,7 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         // learned seeding: the network's guess per anchor under its model
         std::vector<float> anchor_uv;
         bool guided = false;
-        if (learned) {
+        auto learned_guesses = [&]() {
             const auto t_g = clk::now();
             anchor_uv = learned_anchor_guesses(d_def, model_H, params, lat_x, lat_y, solved, gW);
             // the model refitted to where the anchors land under the guesses,
@@ -1135,7 +1161,8 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             E.last_learned_.ms += (float)ms_since(t_g);
             E.last_learned_.anchor_uv = anchor_uv;
             guided = true;
-        }
+        };
+        if (learned) learned_guesses();
 
         auto solve_lattice = [&](bool sim) -> float {
             quality = Quality::NONE;
@@ -1273,9 +1300,9 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         }
         };
         seed_lattice();
-        if (learned) {
-            // the lattice judges the proposal: its error against the anchors
-            // solved under it, and whether the keep rule held
+        // the lattice judges the proposal: its error against the anchors
+        // solved under it, and whether the keep rule held
+        auto judge_learned = [&]() {
             LearnedSeed& Ls = E.last_learned_;
             double se = 0.0;
             for (const Anchor& a : anchors) {
@@ -1289,15 +1316,34 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
             }
             Ls.err_mean = Ls.anchors ? (float)(se / Ls.anchors) : 0.f;
             Ls.kept = have_model && !model_rejected;
-            if (!Ls.kept) {
-                // rejected: seed again from the global-motion estimate, the
-                // anchors' statistics counted for that seeding only
+            return Ls.kept;
+        };
+        // seed again from the global-motion estimate alone, the anchors'
+        // statistics counted for that seeding only
+        auto reseed_plain = [&]() {
+            st_anchor = HostStats();
+            model_H = nullptr;
+            guided = false;
+            plain_estimate();
+            setup_model();
+            seed_lattice();
+        };
+        if (learned) {
+            if (!judge_learned()) reseed_plain();
+        } else if (!caller_model && ref_gray && E.learned_rescue_ && E.proposal_ &&
+                   (model_rejected || (!have_model && quality != Quality::FULL))) {
+            // rescue order: the lattice rejected the estimate's model, or the
+            // estimate did not lock and the plain lattice fell short of full
+            // quality, so the proposal is tried, its seeding judged the same
+            // way; a rejected proposal leaves the run as the estimate seeded it
+            if (learned_model(params, d_def, learned_H)) {
+                learned = true;
                 st_anchor = HostStats();
-                model_H = nullptr;
-                guided = false;
-                plain_estimate();
+                model_H = learned_H;
                 setup_model();
+                learned_guesses();
                 seed_lattice();
+                if (!judge_learned()) reseed_plain();
             }
         }
         // publish_anchor_results (full_field_anchors.cpp:576-607)

@@ -198,14 +198,19 @@ public:
     // The estimate of the last run (locked false: none, or none used).
     const dic::GlobalSimilarity& last_global() const { return last_global_; }
 
-    // Learned seeding: with a proposal network set (not owned) and `learned`
-    // on, a run with no model given proposes its global model from the
-    // network's predictions on patch pairs of the reference and the deformed
-    // frame; the anchor lattice judges it by the reference's keep rule and,
-    // if it is rejected, the run seeds again from the global-motion estimate.
-    void set_proposal(ProposalNet* net, bool learned) {
+    // Learned seeding: with a proposal network set (not owned), a run with no
+    // model given proposes its global model from the network's predictions on
+    // patch pairs of the reference and the deformed frame, and the anchor
+    // lattice judges it by the reference's keep rule. `mode` 1: the proposal
+    // first, and if the lattice rejects it, the global-motion estimate; mode
+    // 2: the global-motion estimate first, and the proposal only when the
+    // estimate does not lock or the lattice rejects its model (if the lattice
+    // rejects the proposal too, the run seeds as from the estimate alone);
+    // 0: off.
+    void set_proposal(ProposalNet* net, int mode) {
         proposal_ = net;
-        learned_ = learned && net != nullptr;
+        learned_ = mode != 0 && net != nullptr;
+        learned_rescue_ = learned_ && mode == 2;
     }
     const LearnedSeed& last_learned() const { return last_learned_; }
 
@@ -240,6 +245,7 @@ private:
     dic::GlobalSimilarity last_global_;
     ProposalNet* proposal_ = nullptr;
     bool learned_ = false;
+    bool learned_rescue_ = false;  // the proposal only where the global-motion estimate fails
     LearnedSeed last_learned_;
     PhaseTimes times_;
     friend struct Impl;

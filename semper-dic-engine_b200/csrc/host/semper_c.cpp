@@ -484,7 +484,8 @@ SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_propos
     if (eng == nullptr) return SEMPER_ERR_INIT;
     HandleCall call(eng->busy);
     if (!call.owned()) return SEMPER_ERR_INIT;
-    eng->engine.set_proposal(p ? p->net.get() : nullptr, learned != 0);
+    if (learned < 0 || learned > 2) return SEMPER_ERR_INIT;
+    eng->engine.set_proposal(p ? p->net.get() : nullptr, learned);
     return 0;
 }
 

@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -2436,13 +2437,20 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
-void tile_box(int dim, int six, int& tw, int& th) {
-    // the subset's support plus one pixel of rounding slack each side, three
-    // columns of alignment slack, and a margin for the warp to move in before
-    // the tile is staged again: two pixels each way across, one up and down
-    // (two rows fewer of shared memory: subset 41's fast pass holds 12 warps
-    // per SM instead of 11)
-    const int need = dim + (six ? 5 : 3) + 2;
+// The support a warped subset needs: the subset's side, grown by `spread`
+// when it is above 1, plus the interpolation taps and a pixel of rounding
+// slack each side.
+static int support_of(int dim, int six, float spread) {
+    const int side = spread > 1.0f ? (int)std::ceil((double)dim * spread) : dim;
+    return side + (six ? 5 : 3) + 2;
+}
+
+void tile_box(int dim, int six, int& tw, int& th, float spread) {
+    // the warped subset's support, three columns of alignment slack, and a
+    // margin for the warp to move in before the tile is staged again: two
+    // pixels each way across, one up and down (two rows fewer of shared
+    // memory: subset 41's fast pass holds 12 warps per SM instead of 11)
+    const int need = support_of(dim, six, spread);
     tw = ((need + 3 + 4) + 3) & ~3;
     th = need + 2;
     if (tw > 256 || th > 256) tw = th = 0;
@@ -2451,14 +2459,14 @@ void tile_box(int dim, int six, int& tw, int& th) {
 // The rescue pass's tile: twice the support each way (capped by the TMA box
 // limit), so the wide warps of Simplex probes and diverging iterations keep
 // reading shared memory; 0 when the fast pass's box is unavailable.
-void rescue_tile_box(int dim, int six, int& tw, int& th) {
+void rescue_tile_box(int dim, int six, int& tw, int& th, float spread = 0.0f) {
     int fw = 0, fh = 0;
-    tile_box(dim, six, fw, fh);
+    tile_box(dim, six, fw, fh, spread);
     if (fw == 0) {
         tw = th = 0;
         return;
     }
-    const int need = dim + (six ? 5 : 3) + 2;
+    const int need = support_of(dim, six, spread);
     tw = std::min(((2 * need + 7) + 3) & ~3, 256);
     th = std::min(2 * need, 256);
 }
@@ -2468,7 +2476,7 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     CUtensorMap tmap;
     std::memset(&tmap, 0, sizeof(tmap));
     int tw = 0, th = 0;
-    tile_box(a.dim, six, tw, th);
+    tile_box(a.dim, six, tw, th, a.tile_spread);
     const bool pitch_ok = (a.pitch % 4) == 0 && (reinterpret_cast<uintptr_t>(a.defI) % 16) == 0;
     PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
     if (tw > 0 && pitch_ok && enc) {
@@ -2489,7 +2497,7 @@ cudaError_t launch_solve(const SolveArgs& a0, int six, int grid_blocks, cudaStre
     std::memset(&tmap_r, 0, sizeof(tmap_r));
     int tw_r = 0, th_r = 0;
     if (tw > 0) {
-        rescue_tile_box(a.dim, six, tw_r, th_r);
+        rescue_tile_box(a.dim, six, tw_r, th_r, a.tile_spread);
         const cuuint64_t gdim[2] = {(cuuint64_t)a.W, (cuuint64_t)a.H};
         const cuuint64_t gstride[1] = {(cuuint64_t)a.pitch * 4};
         const cuuint32_t box[2] = {(cuuint32_t)tw_r, (cuuint32_t)th_r};

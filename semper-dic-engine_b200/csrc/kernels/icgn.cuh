@@ -47,6 +47,11 @@ struct SolveArgs {
     // centred at (cx, cy) is read at (cx + ref_dx, cy + ref_dy) of planes with
     // row pitch ref_pitch (0: the same planes frame, pitch). Staged solver only.
     int ref_pitch, ref_dx, ref_dy;
+    // How far the warped subset's bounding box outgrows the subset (its
+    // side over the subset's, e.g. |cos| + |sin| of a rotation): above 1 the
+    // TMA tiles are sized for it (the fast pass then runs its generic
+    // instance); 0 or 1: the tiles of an unrotated subset.
+    float tile_spread;
 };
 
 struct SmemLayout {
@@ -62,7 +67,7 @@ __host__ __device__ inline SmemLayout smem_layout(int max_n, int tile_w, int til
     L.bytes = (L.off_refok + (size_t)max_n + 127) & ~(size_t)127;
     return L;
 }
-void tile_box(int dim, int six, int& tw, int& th);
+void tile_box(int dim, int six, int& tw, int& th, float spread = 0.0f);
 // Two launches on `st`: the fast pass over every task, then the general pass
 // over the tasks it deferred. Scratch: queue (3 ints) and deferred (n ints).
 cudaError_t launch_solve(const SolveArgs& a, int six, int grid_blocks, cudaStream_t st);

@@ -241,9 +241,10 @@ class Engine:
         return lib().semper_set_reference(self._h, _p(buf, _u8p), buf.size, None, 0, width, height)
 
     def run(self, deformed: np.ndarray, prm: SemperParams, capacity: int | None = None, mask=None,
-            metrics_len: int = 24, progress=None, out: np.ndarray | None = None):
+            metrics_len: int = 24, progress=None, out: np.ndarray | None = None, copy: bool = True):
         """semper_run. `out` (float32, >= capacity) may be a caller buffer,
-        e.g. pinned memory; the returned points are a copy either way."""
+        e.g. pinned memory; the returned points are a copy, or with copy False
+        a view of `out` (valid until `out` is reused)."""
         d = np.ascontiguousarray(deformed, np.uint8)
         m = None if mask is None else np.ascontiguousarray(mask, np.uint8)
         if capacity is None:
@@ -254,7 +255,8 @@ class Engine:
         cb = PROGRESS_CB(progress) if progress else PROGRESS_CB()
         rc = lib().semper_run(self._h, _p(d, _u8p), d.size, _p(m, _u8p), 0 if m is None else m.size,
                               ctypes.byref(prm), _p(out, _f32p), capacity, _p(met, _f32p), metrics_len, cb, None)
-        return rc, out[: max(rc, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy()
+        pts = out[: max(rc, 0) * 8].reshape(-1, 8)
+        return rc, pts.copy() if copy else pts, met[:metrics_len].copy()
 
     def cancel(self):
         lib().semper_cancel(self._h)
@@ -286,10 +288,14 @@ class Engine:
         Hm = None if H is None else np.ascontiguousarray(H, np.float64).reshape(9)
         return lib().semper_b200_set_global_model(self._h, _p(Hm, _f64p))
 
-    def set_proposal(self, net, learned: bool = True) -> int:
-        """Learned seeding from `net` (a Proposal, kept alive by this engine)."""
+    def set_proposal(self, net, learned=True) -> int:
+        """Learned seeding from `net` (a Proposal, kept alive by this engine).
+        learned: True or 1, the proposal first; "rescue" or 2, the
+        global-motion estimate first and the proposal only where it fails;
+        False or 0, off."""
         self._proposal = net
-        return lib().semper_b200_set_proposal(self._h, None if net is None else net._h, 1 if learned else 0)
+        mode = 2 if learned == "rescue" else int(learned)
+        return lib().semper_b200_set_proposal(self._h, None if net is None else net._h, mode)
 
     def last_learned(self) -> dict:
         o = np.zeros(18, np.float64)

@@ -79,3 +79,28 @@ def test_learned_seeding_gain(net, pair):
     assert res["learned"][1] < 0.01
     if res["global"][0] > 0:
         assert res["learned"][0] >= res["global"][0]
+
+
+def test_rescue_order_matches_the_seeding_it_takes(net, pair):
+    """The rescue order (the global-motion estimate first, the proposal only
+    where the lattice rejects the estimate's model): on pair 0, whose estimate
+    the lattice keeps, the field of the estimate alone, with the network never
+    run; on pair 3, whose estimate is off by pixels and rejected, the field of
+    the proposal-first seeding, bit for bit."""
+    k, (ref, dfm, prm, warp, sim) = pair
+    out = {}
+    for mode in ("rescue", "learned", "global"):
+        eng = sb.Engine()
+        assert eng.set_reference(ref) == 0
+        if mode != "global":
+            assert eng.set_proposal(net, "rescue" if mode == "rescue" else True) == 0
+        rc, pts, met = eng.run(dfm, prm)
+        out[mode] = (rc, pts, met, eng.last_learned())
+    rc, pts, met, L = out["rescue"]
+    other = out["global"] if k == 0 else out["learned"]
+    assert rc == other[0] > 0
+    assert np.array_equal(pts, other[1])
+    assert np.array_equal(met[:8], other[2][:8])
+    assert L["ran"] == (k == 3)
+    if k == 3:
+        assert L["kept"] and out["global"][0] <= 0
