@@ -329,6 +329,25 @@ def test_pipeline_target_settings_2048_bit_exact():
     _assert_field_equal(d, o)
 
 
+def test_pipeline_cfg1_4096_bit_exact():
+    """The headline workload itself: cfg1 at 4096^2 (step 4, subset 31, window
+    31; 1,014,049 attempted nodes), the device field against the CPU
+    restatement's, bit for bit."""
+    ref, dfm, prm, _ = sb.config_pair(1)
+    d, o = _run_both(ref, dfm, prm)
+    assert o[0] > 1000000
+    _assert_field_equal(d, o)
+
+
+def test_pipeline_target_settings_4096_bit_exact():
+    """The target settings at their full size: 4096^2, step 8, subset 41,
+    window 41, bit for bit."""
+    ref, dfm, prm, _ = sb.config_pair(4)
+    d, o = _run_both(ref, dfm, prm)
+    assert o[0] > 240000
+    _assert_field_equal(d, o)
+
+
 def test_batch_cfg2_jobs_against_restatement():
     """Eight pairs of the batched uneven workload (masks, rotations, subsets
     15-41, steps 4 and 8), solved in one batch call, each against the CPU
