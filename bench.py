@@ -652,6 +652,9 @@ def run_cfg4_seedings(args, rank):
                 ev1.record(stream)
                 torch.cuda.synchronize()
                 ms = ev0.elapsed_time(ev1)
+                # e2e: one untimed call through semper_run first (its host
+                # path sizes its buffers on first use), then K timed
+                eng.run(h_frame.numpy(), prm, capacity=cap, out=h_out, copy=False)
                 torch.cuda.synchronize()
                 t0 = time.perf_counter()
                 for _ in range(args.steps):

@@ -15,6 +15,9 @@ ProposalNet::ProposalNet(int max_batch) : max_batch_(max_batch) {
     const size_t n = param_count();
     for (DevBuf<float>* b : {&params_, &grads_, &m_, &v_}) b->ensure(n);
     target_.ensure((size_t)max_batch * dic::kPpOut);
+    centres_.ensure((size_t)max_batch * 8);
+    check(cudaHostAlloc(&h_maps_, (size_t)max_batch * 8 * sizeof(float), cudaHostAllocDefault), "pinned maps");
+    check(cudaHostAlloc(&h_out_, (size_t)max_batch * 6 * sizeof(float), cudaHostAllocDefault), "pinned out");
     work_.ensure(dic::pp_work_bytes(max_batch));
     dic::pp_work_carve(w_, work_.p, max_batch);
     init(0);
@@ -25,6 +28,14 @@ ProposalNet::~ProposalNet() {
         cudaStreamSynchronize(st_);
         cudaStreamDestroy(st_);
     }
+    drop_graphs();
+    if (h_maps_) cudaFreeHost(h_maps_);
+    if (h_out_) cudaFreeHost(h_out_);
+}
+
+void ProposalNet::drop_graphs() {
+    for (auto& kv : graphs_) cudaGraphExecDestroy(kv.second);
+    graphs_.clear();
 }
 
 size_t ProposalNet::param_count() { return dic::pp_layout().total; }
@@ -159,12 +170,32 @@ void ProposalNet::predict_warped(const uint8_t* d_ref, const uint8_t* d_def, int
                                  const float* maps, int K, int f, float* out, cudaStream_t st) {
     if (K <= 0 || K > max_batch_) throw std::invalid_argument("proposal: batch");
     if (W < 2 || H < 2 || pitch < W || f < 1 || f > 16) throw std::invalid_argument("proposal: frame or factor");
-    centres_.ensure(std::max(centres_.n, (size_t)K * 8));
-    check(cudaMemcpyAsync(centres_.p, maps, (size_t)K * 32, cudaMemcpyHostToDevice, st), "H2D maps");
-    check(dic::pp_cut_warped(d_ref, d_def, W, H, pitch, centres_.p, K, f, w_.act[0], w_.y, st), "cut warped");
-    check(dic::pp_forward(params_.p, w_, K, st), "proposal forward");
-    check(cudaMemcpyAsync(out, w_.out, (size_t)K * 6 * 4, cudaMemcpyDeviceToHost, st), "D2H out");
+    // one graph launch instead of 16 launches and two pageable copies: the
+    // cascade of the learned seeding makes about a dozen of these calls a
+    // frame, each waiting for its predictions
+    std::memcpy(h_maps_, maps, (size_t)K * 32);
+    const GraphKey key{d_ref, d_def, W, H, pitch, K, f, st};
+    auto it = graphs_.find(key);
+    if (it == graphs_.end()) {
+        if (graphs_.size() >= 64) drop_graphs();
+        cudaGraph_t g = nullptr;
+        check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "capture");
+        cudaError_t e = cudaMemcpyAsync(centres_.p, h_maps_, (size_t)K * 32, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = dic::pp_cut_warped(d_ref, d_def, W, H, pitch, centres_.p, K, f, w_.act[0], w_.y, st);
+        if (e == cudaSuccess) e = dic::pp_forward(params_.p, w_, K, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_out_, w_.out, (size_t)K * 6 * 4, cudaMemcpyDeviceToHost, st);
+        const cudaError_t ee = cudaStreamEndCapture(st, &g);
+        check(e, "proposal capture");
+        check(ee, "capture end");
+        cudaGraphExec_t x = nullptr;
+        e = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        check(e, "graph instantiate");
+        it = graphs_.emplace(key, x).first;
+    }
+    check(cudaGraphLaunch(it->second, st), "graph launch");
     check(cudaStreamSynchronize(st), "sync");
+    std::memcpy(out, h_out_, (size_t)K * 6 * 4);
 }
 
 void ProposalNet::predict_warped_host(const uint8_t* ref, const uint8_t* def, int W, int H, const float* maps, int K,

@@ -5,6 +5,8 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -62,6 +64,24 @@ private:
     DevBuf<unsigned char> work_, frames_;
     dic::PpWork w_;
     int adam_t_ = 0;
+    // predict_warped as one CUDA graph per (frames, size, batch, factor,
+    // stream): the map upload from pinned staging, the patch cut, the
+    // forward and the prediction download, captured on first use. The
+    // graphs hold the device buffers' addresses, which stay fixed (centres_
+    // is sized for max_batch up front).
+    struct GraphKey {
+        const void* ref;
+        const void* def;
+        int W, H, pitch, K, f;
+        cudaStream_t st;
+        bool operator<(const GraphKey& o) const {
+            return std::tie(ref, def, W, H, pitch, K, f, st) < std::tie(o.ref, o.def, o.W, o.H, o.pitch, o.K, o.f, o.st);
+        }
+    };
+    std::map<GraphKey, cudaGraphExec_t> graphs_;
+    float* h_maps_ = nullptr;  // pinned, max_batch x 8
+    float* h_out_ = nullptr;   // pinned, max_batch x 6
+    void drop_graphs();
 };
 
 }  // namespace semper_b200
