@@ -452,7 +452,9 @@ class Batch:
             cap = j.get("capacity")
             if cap is None:
                 cap = max(prm.rect_w // max(prm.step, 1), 1) * max(prm.rect_h // max(prm.step, 1), 1) * 8
-            out = np.zeros(max(cap, 1), np.float32)
+            # fresh per call and written by the library up to the point count,
+            # so neither zeroed nor copied on the way out
+            out = np.empty(max(cap, 1), np.float32)
             met = np.zeros(max(metrics_len, 1), np.float32)
             keep += [ref, dfm, m, out, met]
             outs.append((out, met))
@@ -471,7 +473,7 @@ class Batch:
         res = []
         for k, (out, met) in enumerate(outs):
             r = arr[k].result
-            res.append((r, out[: max(r, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy()))
+            res.append((r, out[: max(r, 0) * 8].reshape(-1, 8), met[:metrics_len]))
         return res
 
 
@@ -637,7 +639,7 @@ class IncrementalBatch:
         keep = []
         for i, q in enumerate(seqs):
             d = np.ascontiguousarray(frames[q], np.uint8)
-            out = np.zeros(max(capacity, 1), np.float32)
+            out = np.empty(max(capacity, 1), np.float32)  # fresh per call: returned as views
             met = np.zeros(max(metrics_len, 1), np.float32)
             keep.append((d, out, met))
             arr[i].sequence = q
@@ -655,7 +657,7 @@ class IncrementalBatch:
             _, out, met = keep[i]
             info = IncrementalInfo()
             ctypes.memmove(ctypes.byref(info), ctypes.byref(arr[i].info), ctypes.sizeof(IncrementalInfo))
-            res[q] = (r, out[: max(r, 0) * 8].reshape(-1, 8).copy(), met[:metrics_len].copy(), info)
+            res[q] = (r, out[: max(r, 0) * 8].reshape(-1, 8), met[:metrics_len], info)
         return res
 
 
