@@ -2108,8 +2108,9 @@ __device__ __forceinline__ void solver_setup(WarpSolver<SIX, Mask, STAGE, COOP>&
 // bookkeeping folds away; 32-bit validity masks up to 32 pixels per lane.
 // Subset 41's tile and sampled values (18.7 KB a warp) leave room for 12
 // warps per SM, so its registers are capped for 12 (no spills), the others'
-// for 18.
-template <bool SIX, int DIMC, bool STAGE>
+// for 18. RT: the tile box taken from the launch (a box sized for a rotated
+// or stretched subset) with the subset size still known at compile time.
+template <bool SIX, int DIMC, bool STAGE, bool RT = false>
 __global__ void __launch_bounds__(32, (DIMC == 41 ? 12 : 18)) fast_kernel(const __grid_constant__ CUtensorMap tmap, const SolveArgs a,
                                                   const StagedLayout L) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -2118,7 +2119,8 @@ __global__ void __launch_bounds__(32, (DIMC == 41 ? 12 : 18)) fast_kernel(const 
     constexpr int kTh = DIMC > 0 ? DIMC + (SIX ? 5 : 3) + 2 + 2 : 0;
     WarpSolver<SIX, Mask, STAGE> s;
     solver_setup(s, smem, L, &tmap, a.refI, a.refGx, a.refGy, a.defI, a.err, DIMC > 0 ? DIMC * DIMC : a.n,
-                 DIMC > 0 ? DIMC : a.dim, a.pitch, DIMC > 0 ? kTw : a.tile_w, DIMC > 0 ? kTh : a.tile_h, a.W, a.H,
+                 DIMC > 0 ? DIMC : a.dim, a.pitch, (DIMC > 0 && !RT) ? kTw : a.tile_w,
+                 (DIMC > 0 && !RT) ? kTh : a.tile_h, a.W, a.H,
                  a.min_valid, a.lm, a.ref_pitch, a.ref_dx, a.ref_dy, a.tma_max_polls);
     if (DIMC > 0) s.tile_on = a.tile_w > 0;
     s.no_ghost = a.ref_no_ghost != 0;
@@ -2391,6 +2393,13 @@ cudaError_t launch_passes(const CUtensorMap& tmap, const CUtensorMap& tmap_r, in
         if (box_ok && a.dim == 21) fast = stage ? fast_kernel<SIX, 21, true> : fast_kernel<SIX, 21, false>;
         if (box_ok && a.dim == 31) fast = stage ? fast_kernel<SIX, 31, true> : fast_kernel<SIX, 31, false>;
         if (box_ok && a.dim == 41) fast = stage ? fast_kernel<SIX, 41, true> : fast_kernel<SIX, 41, false>;
+        // a box sized for a rotated subset (the seeding model's spread): the
+        // compile-time subset size with the launch's box
+        if (!box_ok && !stage && a.tile_w > 0) {
+            if (a.dim == 21) fast = fast_kernel<SIX, 21, false, true>;
+            if (a.dim == 31) fast = fast_kernel<SIX, 31, false, true>;
+            if (a.dim == 41) fast = fast_kernel<SIX, 41, false, true>;
+        }
         const StagedLayout FL = staged_layout(a.n, a.tile_w, a.tile_h, stage);
         if (!a.rescue_all) {
             e = allow_max_smem(fast);
