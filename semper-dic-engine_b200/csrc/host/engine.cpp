@@ -599,6 +599,10 @@ struct Engine::Impl {
     // |J10| + |J11|) (J the model's local linear map at the ROI centre), and
     // the tiles grow with it, 4 % beyond for the field's own variation.
     // Below 1.03 the tiles of an unrotated subset serve.
+    // the last Delaunay triangulation of the mesh guess and its points
+    std::vector<semper_geom::Pt> dl_pts;
+    std::vector<semper_geom::Tri> dl_tris;
+
     float tile_spread = 0.f;
     void set_tile_spread(const double* H, const Params& p) {
         tile_spread = 0.f;
@@ -1390,7 +1394,17 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
                     ins.push_back(ref_pts[i]);
                     ins_of.push_back((int)i);
                 }
-            for (const semper_geom::Tri& t : semper_geom::delaunay(ins)) {
+            // the triangulation depends on the points alone: a frame whose
+            // kept anchors sit where the last one's did (a fixed reference,
+            // an incremental sequence's lattice) reuses it
+            if (ins.size() != dl_pts.size() ||
+                !std::equal(ins.begin(), ins.end(), dl_pts.begin(), [](const semper_geom::Pt& a, const semper_geom::Pt& b) {
+                    return a.x == b.x && a.y == b.y;
+                })) {
+                dl_tris = semper_geom::delaunay(ins);
+                dl_pts = ins;
+            }
+            for (const semper_geom::Tri& t : dl_tris) {
                 dic::MeshTri mt;
                 semper_geom::Pt src[3], dst[3];
                 const int vi[3] = {t.a, t.b, t.c};
