@@ -696,6 +696,7 @@ struct Engine::Impl {
 
     // the material-mask warp of incremental DIC
     DevBuf<uint8_t> mMask0, mOut, mTmp;
+    size_t mMask0_px = 0;  // pixels of the material mask last uploaded to mMask0
     DevBuf<float> mU, mV;
     DevBuf<int> mBox;
 
@@ -783,7 +784,7 @@ int Engine::set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask
     return 0;
 }
 
-int Engine::adopt_last_deformed(const uint8_t* mask) {
+int Engine::adopt_last_deformed(const uint8_t* mask, bool mask_on_device) {
     Impl& I = *impl_;
     if (!has_ref_ || !I.dI.p) return -3;
     std::swap(I.rI.p, I.dI.p);
@@ -804,8 +805,10 @@ int Engine::adopt_last_deformed(const uint8_t* mask) {
         // Ghost Wall on the adopted frame: the gradients stay those of the
         // real intensities (stamp after prepare, reference_cache.cpp:95-96).
         const size_t n = (size_t)W_ * H_;
-        I.mOut.ensure(std::max(I.mOut.n, n));
-        check(cudaMemcpyAsync(I.mOut.p, mask, n, cudaMemcpyHostToDevice, stream_), "H2D mask");
+        if (!(mask_on_device && I.mOut.p && I.mOut.n >= n)) {
+            I.mOut.ensure(std::max(I.mOut.n, n));
+            check(cudaMemcpyAsync(I.mOut.p, mask, n, cudaMemcpyHostToDevice, stream_), "H2D mask");
+        }
         I.launched(1, dic::launch_stamp_ghost(I.rI.p, W_, H_, (W_ + 3) & ~3, I.mOut.p, stream_), "ghost stamp");
         check(cudaStreamSynchronize(stream_), "sync");
     }
@@ -835,18 +838,23 @@ int check_params(Params& p, int width, int height) { return validate_params(p, w
 
 int Engine::warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, int rect_x, int rect_y, int step,
                       const float* U, const float* V, int X0, int X1, int Y0, int Y1, int per_px, uint8_t* out,
-                      int box[4]) {
+                      int box[4], bool mask0_resident) {
     Impl& I = *impl_;
     if (!mask0 || !U || !V || !out || W <= 0 || H <= 0 || gridW <= 0 || gridH <= 0 || step <= 0) return -3;
     cudaStream_t st = stream_;
     const size_t n = (size_t)W * H, ng = (size_t)gridW * gridH;
+    // the material mask of frame 0 stays on the device between calls
+    mask0_resident = mask0_resident && I.mMask0.p && I.mMask0_px == n;
     I.mMask0.ensure(std::max(I.mMask0.n, n));
     I.mOut.ensure(std::max(I.mOut.n, n));
     I.mTmp.ensure(std::max(I.mTmp.n, n));
     I.mU.ensure(std::max(I.mU.n, ng));
     I.mV.ensure(std::max(I.mV.n, ng));
     I.mBox.ensure(4);
-    check(cudaMemcpyAsync(I.mMask0.p, mask0, n, cudaMemcpyHostToDevice, st), "H2D material mask");
+    if (!mask0_resident) {
+        check(cudaMemcpyAsync(I.mMask0.p, mask0, n, cudaMemcpyHostToDevice, st), "H2D material mask");
+        I.mMask0_px = n;
+    }
     check(cudaMemcpyAsync(I.mU.p, U, ng * 4, cudaMemcpyDefault, st), "copy U");
     check(cudaMemcpyAsync(I.mV.p, V, ng * 4, cudaMemcpyDefault, st), "copy V");
     const dic::MaskField f{gridW, gridH, rect_x, rect_y, step, I.mU.p, I.mV.p};

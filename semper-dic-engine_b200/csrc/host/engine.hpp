@@ -141,8 +141,10 @@ public:
     int set_reference(const uint8_t* gray, int w, int h, const uint8_t* mask);
     // The deformed frame of the last solve becomes the reference
     // (ReferenceCache::adopt, src/pipeline/reference_cache.cpp:82-108): its
-    // prepared planes are taken over on the device.
-    int adopt_last_deformed(const uint8_t* mask);
+    // prepared planes are taken over on the device. mask_on_device: the mask
+    // is the one the last warp_mask call left on the device (not uploaded
+    // again).
+    int adopt_last_deformed(const uint8_t* mask, bool mask_on_device = false);
     void reset();
     bool has_reference() const { return has_ref_; }
     int width() const { return W_; }
@@ -180,9 +182,10 @@ public:
     // [X0, X1] x [Y0, Y1] sends per_px x per_px samples X to X + U(X), U the
     // filled field of the grid; then a 3x3 close. out (host, W x H) receives
     // the mask; box = {x, y, w, h} of its nonzero pixels (all 0 if none).
+    // mask0_resident: mask0 is the one the last call uploaded, unchanged.
     int warp_mask(const uint8_t* mask0, int W, int H, int gridW, int gridH, int rect_x, int rect_y, int step,
                   const float* U, const float* V, int X0, int X1, int Y0, int Y1, int per_px, uint8_t* out,
-                  int box[4]);
+                  int box[4], bool mask0_resident = false);
 
     void request_cancel() { h_cancel_[0] = 1; }
     void clear_cancel() { h_cancel_[0] = 0; }

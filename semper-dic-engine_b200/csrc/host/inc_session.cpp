@@ -112,6 +112,8 @@ struct IncrementalSession::Impl {
     int interval = 0;
     int W = 0, H = 0;
     std::vector<uint8_t> user_mask0, material0;
+    bool material0_on_device = false;  // the engine holds material0 since the last mask warp
+    std::vector<uint8_t> spare_mask;   // a W x H buffer for the next warped mask
     dic::IncGrid g0{};
     int n0 = 0;
     int frame0_points = -1;
@@ -143,6 +145,7 @@ struct IncrementalSession::Impl {
         W = H = 0;
         user_mask0.clear();
         material0.clear();
+        material0_on_device = false;
         g0 = dic::IncGrid{};
         n0 = 0;
         frame0_points = -1;
@@ -215,6 +218,7 @@ int IncrementalSession::Impl::init(const uint8_t* ref, int w, int h, const uint8
         user_mask0.assign(roi_mask, roi_mask + npx);
         material0.resize(npx);
         for (size_t i = 0; i < npx; ++i) material0[i] = roi_mask[i] >= 128 ? 255 : 0;
+        material0_on_device = false;
     } else {
         // the ROI rect widened by the reach of its edge nodes' subsets at 45 deg
         const int reach = (int)std::ceil(params.subset_size / 2 * std::sqrt(2.0)) + 1;
@@ -223,6 +227,7 @@ int IncrementalSession::Impl::init(const uint8_t* ref, int w, int h, const uint8
                                   params.rect_h + 2 * reach},
                               Box{0, 0, W, H});
         for (int y = r.y; y < r.y + r.h; ++y) std::memset(material0.data() + (size_t)y * W + r.x, 255, (size_t)r.w);
+        material0_on_device = false;
     }
     if (engine.set_reference(ref, W, H, user_mask0.empty() ? nullptr : user_mask0.data()) != 0) {
         clear();
@@ -296,9 +301,12 @@ bool IncrementalSession::Impl::warp_mask(const uint8_t* alive_flags, const float
     check(dic::launch_inc_fill_init(n0, Ut, Vt, alive_flags, fillU[0].p, fillV[0].p, filled[0].p, counters.p, st()),
           "fill init");
     counters_to_host(&any, 13, 1);
-    out.assign((size_t)W * H, 0);
+    // every byte is written below: zeros on the early returns, the device's
+    // mask otherwise (so a recycled buffer is not cleared first)
+    if (out.size() != (size_t)W * H) out.assign((size_t)W * H, 0);
     bb = Box{};
     if (!any) {
+        std::fill(out.begin(), out.end(), 0);
         prof.warp_mask += ms_since(t0);
         return false;
     }
@@ -331,12 +339,15 @@ bool IncrementalSession::Impl::warp_mask(const uint8_t* alive_flags, const float
     const int X0 = std::max(0, g0.rect_x - margin), X1 = std::min(W - 1, g0.rect_x + (g0.gw - 1) * g0.step + margin);
     const int Y0 = std::max(0, g0.rect_y - margin), Y1 = std::min(H - 1, g0.rect_y + (g0.gh - 1) * g0.step + margin);
     if (X0 > X1 || Y0 > Y1) {
+        std::fill(out.begin(), out.end(), 0);
         prof.warp_mask += ms_since(t0);
         return false;
     }
     int box[4] = {0, 0, 0, 0};
+    const bool resident = material0_on_device;
+    material0_on_device = true;
     if (engine.warp_mask(material0.data(), W, H, g0.gw, g0.gh, g0.rect_x, g0.rect_y, g0.step, fillU[cur].p,
-                         fillV[cur].p, X0, X1, Y0, Y1, per_px, out.data(), box) != 0)
+                         fillV[cur].p, X0, X1, Y0, Y1, per_px, out.data(), box, resident) != 0)
         throw std::runtime_error("mask warp");
     bb = Box{box[0], box[1], box[2], box[3]};
     prof.warp_mask += ms_since(t0);
@@ -500,9 +511,9 @@ int IncrementalSession::Impl::process(const uint8_t* def, float* out, int capaci
 
     // the next reference: the warped material mask, and the rect that holds
     // every followed node (widened by a step) inside the frame
-    std::vector<uint8_t> next_mask;
+    std::vector<uint8_t> next_mask = std::move(spare_mask);  // the buffer of the mask before last
     Box bb;
-    warp_mask(alive_next.p, U.p, V.p, next_mask, bb);
+    const bool warped = warp_mask(alive_next.p, U.p, V.p, next_mask, bb);
     Params next = params;
     Box grid_rect;
     if (alive_new > 0) {
@@ -522,7 +533,8 @@ int IncrementalSession::Impl::process(const uint8_t* def, float* out, int capaci
         alive_new = 0;
     }
     const auto t2 = std::chrono::steady_clock::now();
-    if (engine.adopt_last_deformed(next_mask.data()) != 0) return -3;
+    // the warped mask is still on the device where the warp left it
+    if (engine.adopt_last_deformed(next_mask.data(), warped) != 0) return -3;
     prof.adopt += ms_since(t2);
 
     // anchors: drop, then cut the refreshed ones on the frame just adopted
@@ -548,7 +560,8 @@ int IncrementalSession::Impl::process(const uint8_t* def, float* out, int capaci
     std::swap(travel.p, travel_next.p);
     std::swap(travel.n, travel_next.n);
     alive_nodes = alive_new;
-    mask_k = std::move(next_mask);
+    std::swap(mask_k, next_mask);
+    spare_mask = std::move(next_mask);
     params_k = next;
     frames++;
     ref_index = frames;
