@@ -1009,10 +1009,13 @@ int Engine::Impl::run(const uint8_t* d_def, const uint8_t* mask, Params params, 
         const auto t_prepass = clk::now();
         // the cached grid and pool hold for this mask (compared in place: no copy on a hit)
         const size_t mask_n = mask ? (size_t)W * H : 0;
-        const bool same_mask = mask_key.size() == mask_n && (mask_n == 0 || std::memcmp(mask_key.data(), mask, mask_n) == 0);
+        // the mask compared last, and only when everything else matches (a
+        // reference just adopted rebuilds the grid without comparing)
         const bool cached = grid_valid && key.rect_x == params.rect_x && key.rect_y == params.rect_y &&
                             key.rect_w == params.rect_w && key.rect_h == params.rect_h && key.step == params.step &&
-                            key.subset_size == params.subset_size && same_mask && gridW == gW && gridH == gH;
+                            key.subset_size == params.subset_size && gridW == gW && gridH == gH &&
+                            mask_key.size() == mask_n &&
+                            (mask_n == 0 || std::memcmp(mask_key.data(), mask, mask_n) == 0);
         if (!cached) {
             grid_valid = false;
             skip.ensure(NG);
