@@ -122,3 +122,22 @@ def test_injected_model_takes_precedence():
     assert not e.last_global_motion()["locked"]  # no estimate ran
     orc, opts, _ = _oracle_run(ref, dfm, prm, H)
     assert rc == orc > 0 and np.array_equal(pts, opts)
+
+
+@pytest.mark.parametrize("subset,six", [(21, False), (31, True)])
+def test_rotated_field_other_subsets_and_keys6(subset, six):
+    """The tiles sized for the model's rotation (about 1.4 times the subset
+    side at 45 deg) with the other compiled subset sizes and with the 6x6 Keys
+    interpolator: the field bit-identical to the restatement's under the same
+    model."""
+    ref, dfm, prm0, warp, _sim = sb.large_motion_pair(1024, angle_deg=45.0)
+    prm = sb.params((prm0.rect_x, prm0.rect_y, prm0.rect_w, prm0.rect_h), 8, subset, subset, six=six)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    rc, pts, met = e.run(dfm, prm)
+    g = e.last_global_motion()
+    assert g["locked"]
+    orc, opts, omet = _oracle_run(ref, dfm, prm, g["H"])
+    assert rc == orc and rc > 0.8 * (prm.rect_w // prm.step) ** 2
+    assert np.array_equal(pts, opts)
+    assert np.array_equal(met[COUNT_SLOTS], omet[COUNT_SLOTS])
