@@ -139,3 +139,29 @@ def test_two_gloo_ranks_shard_a_batch_and_solve_it():
     costs = [sb.job_cost(p) for p, _ in sb.batch_job_params(8, seed=5, min_side=160, max_side=288)]
     loads = [sum(costs[g[0]] for g in r[1]) for r in res]
     assert max(loads) <= sum(costs) / 2 + max(costs)
+
+
+def test_shard_covers_every_job_once_and_balances():
+    """semper_b200.shard: every index on exactly one rank, the same split on
+    every call, the largest jobs spread first (no rank above the mean by more
+    than the largest job); batch_jobs with `only` draws the same jobs."""
+    sys.path.insert(0, os.path.join(REPO, "semper-dic-engine_b200"))
+    import semper_b200 as sb
+
+    jobs = sb.batch_job_params(256, seed=0)
+    costs = [sb.job_cost(p) for p, _ in jobs]
+    for world in (1, 2, 3, 8):
+        parts = [sb.shard(costs, r, world) for r in range(world)]
+        assert sorted(sum(parts, [])) == list(range(256))
+        assert parts == [sb.shard(costs, r, world) for r in range(world)]
+        loads = [sum(costs[i] for i in p) for p in parts]
+        assert max(loads) <= sum(costs) / world + max(costs)
+    few = sb.batch_jobs(6, seed=2, min_side=64, max_side=96)
+    some = sb.batch_jobs(6, seed=2, min_side=64, max_side=96, only=[4, 1])
+    assert [j["index"] for j in some] == [1, 4]
+    for j in some:
+        k = j["index"]
+        assert np.array_equal(j["ref"], few[k]["ref"]) and np.array_equal(j["dfm"], few[k]["dfm"])
+        assert (j["mask"] is None) == (few[k]["mask"] is None)
+    assert [m for _, m in sb.batch_job_params(6, seed=2, min_side=64, max_side=96)] == \
+        [j["mask"] is not None for j in few]
