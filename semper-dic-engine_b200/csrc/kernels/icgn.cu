@@ -1275,12 +1275,13 @@ struct WarpSolver {
                     const float2 W0 = f2(Wp[0]), W1 = f2(Wp[1]), W2 = f2(Wp[2]);
                     const float2 W3 = f2(Wp[3]), W4 = f2(Wp[4]), W5 = f2(Wp[5]);
                     const int bx = cx - tx0, by = cy - ty0;
-                    for (int k0 = 0; k0 < K; k0 += 4) {
-                        float v[4], ox[4], oy[4];
-                        int ii[4];
-                        bool ok[4];
+                    constexpr int PG = 8;  // pixels in flight per lane
+                    for (int k0 = 0; k0 < K; k0 += PG) {
+                        float v[PG], ox[PG], oy[PG];
+                        int ii[PG];
+                        bool ok[PG];
 #pragma unroll
-                        for (int u = 0; u < 4; ++u) {
+                        for (int u = 0; u < PG; ++u) {
                             const int k = k0 + u;
                             ii[u] = lane + 32 * k;
                             ok[u] = k < K && ii[u] < n;
@@ -1289,7 +1290,7 @@ struct WarpSolver {
                             advance(row, col);
                         }
 #pragma unroll
-                        for (int u = 0; u < 4; u += 2) {
+                        for (int u = 0; u < PG; u += 2) {
                             const float2 OX = make_float2(ox[u], ox[u + 1]), OY = make_float2(oy[u], oy[u + 1]);
                             const float2 FX = __ffma2_rn(W0, OX, __ffma2_rn(W1, OY, W2));
                             const float2 FY = __ffma2_rn(W3, OX, __ffma2_rn(W4, OY, W5));
@@ -1303,7 +1304,7 @@ struct WarpSolver {
                             v[u + 1] = V.y;
                         }
 #pragma unroll
-                        for (int u = 0; u < 4; ++u)
+                        for (int u = 0; u < PG; ++u)
                             if (ok[u]) {
                                 part = part + v[u];
                                 vals[ii[u]] = v[u];
