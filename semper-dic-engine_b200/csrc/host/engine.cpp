@@ -598,7 +598,9 @@ struct Engine::Impl {
     // subset's bounding box outgrows the subset by max(|J00| + |J01|,
     // |J10| + |J11|) (J the model's local linear map at the ROI centre), and
     // the tiles grow with it, 4 % beyond for the field's own variation.
-    // Below 1.03 the tiles of an unrotated subset serve.
+    // Below 1.03 the tiles of an unrotated subset serve; the spread is capped
+    // at 1.5 (any rotation), so a model that stretches further (a zoom) keeps
+    // tiles that fit shared memory, its outer samples read global memory.
     // the last Delaunay triangulation of the mesh guess and its points
     std::vector<semper_geom::Pt> dl_pts;
     std::vector<semper_geom::Tri> dl_tris;
@@ -610,7 +612,7 @@ struct Engine::Impl {
         double X, Y, J[4];
         if (!semper_geom::homography_at(H, p.rect_x + 0.5 * p.rect_w, p.rect_y + 0.5 * p.rect_h, X, Y, J)) return;
         const double g = std::max(std::fabs(J[0]) + std::fabs(J[1]), std::fabs(J[2]) + std::fabs(J[3]));
-        if (std::isfinite(g) && g > 1.03) tile_spread = (float)std::min(1.04 * g, 4.0);
+        if (std::isfinite(g) && g > 1.03) tile_spread = (float)std::min(1.04 * g, 1.5);
     }
 
     int solve_grid(int ntasks) {

@@ -185,6 +185,7 @@ void ProposalNet::predict_warped(const uint8_t* d_ref, const uint8_t* d_def, int
         if (e == cudaSuccess) e = dic::pp_forward(params_.p, w_, K, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_out_, w_.out, (size_t)K * 6 * 4, cudaMemcpyDeviceToHost, st);
         const cudaError_t ee = cudaStreamEndCapture(st, &g);
+        if ((e != cudaSuccess || ee != cudaSuccess) && g) cudaGraphDestroy(g);
         check(e, "proposal capture");
         check(ee, "capture end");
         cudaGraphExec_t x = nullptr;

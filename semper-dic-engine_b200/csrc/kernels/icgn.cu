@@ -2451,6 +2451,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // when it is above 1, plus the interpolation taps and a pixel of rounding
 // slack each side.
 static int support_of(int dim, int six, float spread) {
+    // at most 1.5 (any rotation): larger spreads keep the tiles of 1.5, so
+    // that both passes' tiles fit shared memory and the TMA box limit
+    spread = std::min(spread, 1.5f);
     const int side = spread > 1.0f ? (int)std::ceil((double)dim * spread) : dim;
     return side + (six ? 5 : 3) + 2;
 }

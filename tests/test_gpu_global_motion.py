@@ -141,3 +141,24 @@ def test_rotated_field_other_subsets_and_keys6(subset, six):
     assert rc == orc and rc > 0.8 * (prm.rect_w // prm.step) ** 2
     assert np.array_equal(pts, opts)
     assert np.array_equal(met[COUNT_SLOTS], omet[COUNT_SLOTS])
+
+
+def test_zoomed_field_tiles_capped():
+    """A 1.8x zoom: the model's spread (1.87 with the margin) is above the
+    tiles' cap of 1.5, so the tiles stay those of 1.5 (inside shared memory
+    and the TMA box limit) and the outer samples read global memory; the
+    field is bit-identical to the restatement's under the same model."""
+    n = 768
+    ref = sb.speckle(n, n, 515)
+    warp = sb.warp_block(cx=n / 2, cy=n / 2, a=(0.8, 0.0, 0.0, 0.8))
+    dfm = sb.speckle(n, n, 515, warp, 1.0, 77)
+    prm = sb.params((288, 288, 192, 192), 8, 21, 21)
+    e = sb.Engine()
+    assert e.set_reference(ref) == 0
+    H = np.array([[1.8, 0.0, -0.8 * n / 2], [0.0, 1.8, -0.8 * n / 2], [0.0, 0.0, 1.0]])
+    assert e.set_global_model(H) == 0
+    rc, pts, met = e.run(dfm, prm)
+    orc, opts, omet = _oracle_run(ref, dfm, prm, H)
+    assert rc == orc and rc > 100
+    assert np.array_equal(pts, opts)
+    assert np.array_equal(met[COUNT_SLOTS], omet[COUNT_SLOTS])
