@@ -214,7 +214,9 @@ SEMPER_C_API int semper_b200_proposal_predict_warped(semper_b200_proposal* p, co
    not lock (and the plain lattice falls short of full quality) or the lattice
    rejects its model, and a rejected proposal leaving the run as the estimate
    seeded it; 0: off. The network must stay alive while the handle may use
-   it. Returns 0, or -3 for a NULL or busy handle or another mode. */
+   it, and serves one run at a time (handles that share a network must not
+   run at once: its buffers are reused by every call). Returns 0, or -3 for
+   a NULL or busy handle or another mode. */
 SEMPER_C_API int semper_b200_set_proposal(semper_engine* eng, semper_b200_proposal* p, int learned);
 
 /* The last run's learned seeding: out[0] 1 when it ran, [1] a model was
